@@ -1,0 +1,370 @@
+"""Benchmark: fold-3 reproBLAS_ddot at N = 2^28 (FP64), the reproducible binned dot product.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one reproducible dot product of two 2^28-element FP64 vectors (uniform(-1,1),
+seeded). Prints ONE JSON line on rank 0.
+
+  value   device throughput in GB/s of algorithmic traffic (16 B per element), inputs
+          resident in HBM, timed with CUDA events over exactly K launches of
+          binnedBLAS_dbddot (2 x 2 GiB inputs, far larger than the 126 MB L2, so no flush
+          is needed between steps); whole job = sum over ranks / max rank time.
+  e2e     the same metric through the reference-facing call reproBLAS_rddot with pinned
+          HOST buffers: every step copies the 4 GiB of inputs to the GPU (staged chunks
+          overlapped with the kernels) and reads the 8-byte result back.
+  roofline  the dominant kernel (the ddot reduction): algorithmic bytes per launch over
+          its mean CUDA-event duration, against the measured HBM copy bandwidth.
+  cpu_baseline  the ReproBLAS reference library (oracle/_ref, compiled from its own
+          sources) on this host's cores: contiguous chunks, one thread each calling
+          binnedBLAS_dbddot, merged with binned_dbdbadd (the reference's own MPI pattern),
+          bit-identical to the single call.
+
+--impl reference times that reference CPU path alone (rank 0; other ranks exit).
+Multi-GPU (torchrun, --gpus N): weak scaling, each rank reduces its own 2^28 shard; the
+per-rank binned states (48 bytes) are all-gathered over NCCL and merged on every GPU.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "ddot GB/s (% HBM peak) at N=2^28 fold 3"
+FOLD = 3
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--log2n", type=int, default=28)
+    p.add_argument("--e2e-steps", type=int, default=5)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def make_inputs(n, rank):
+    rng = np.random.default_rng(2024 + rank)
+    x = rng.uniform(-1.0, 1.0, n)
+    y = rng.uniform(-1.0, 1.0, n)
+    return x, y
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [v.strip() for v in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_dot(R, x, y, threads):
+    """Reference binnedBLAS_dbddot over `threads` contiguous chunks in parallel (ctypes
+    releases the GIL), merged with binned_dbdbadd. Returns (seconds, state)."""
+    from _ffi import ptr, binned_zeros
+    n = len(x)
+    bounds = np.linspace(0, n, threads + 1).astype(np.int64)
+    states = [binned_zeros(FOLD) for _ in range(threads)]
+    xs = x.ctypes.data
+    ys = y.ctypes.data
+    import ctypes
+
+    def work(i):
+        a, b = int(bounds[i]), int(bounds[i + 1])
+        R.dbddot(FOLD, b - a, ctypes.c_void_p(xs + 8 * a), 1, ctypes.c_void_p(ys + 8 * a), 1,
+                 ptr(states[i]))
+
+    R.dbdsum(FOLD, 1, ptr(np.zeros(1)), 1, ptr(binned_zeros(FOLD)))   # builds the bins table
+    t0 = time.perf_counter()
+    ts = [threading.Thread(target=work, args=(i,)) for i in range(threads)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    total = binned_zeros(FOLD)
+    for s in states:
+        R.dbdbadd(FOLD, ptr(s), ptr(total))
+    dt = time.perf_counter() - t0
+    return dt, total
+
+
+def reference_arm(args, rank):
+    from _ffi import ref
+    if rank != 0:
+        return
+    R = ref()
+    if R is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libreproblas_ref.so "
+                          "not built (make -C oracle ref needs the ReproBLAS source tree)"}))
+        return
+    n = 1 << args.log2n
+    x, y = make_inputs(n, 0)
+    threads = host_threads()
+    for _ in range(max(1, min(args.warmup, 2))):
+        cpu_reference_dot(R, x, y, threads)
+    times = [cpu_reference_dot(R, x, y, threads)[0] for _ in range(args.steps)]
+    t = statistics.mean(times)
+    gbs = 16.0 * n / t / 1e9
+    print(json.dumps({
+        "metric": METRIC, "value": round(gbs, 3), "unit": "GB/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(t * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic uniform(-1,1), seed 2024",
+        "config": {"workload": "reproBLAS_ddot fold 3, N=2^%d FP64 (binnedBLAS_dbddot per "
+                               "thread chunk + binned_dbdbadd merge)" % args.log2n,
+                   "n": n, "fold": FOLD},
+        "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": threads,
+                         "kind": "reference",
+                         "sample": "full workload, %d threads, mean of %d steps" % (threads, args.steps)},
+        "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }))
+
+
+def ours_arm(args, rank, world, local_rank):
+    import torch
+    import reproblas_b200 as rb
+    from _ffi import ptr as nptr
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    n = 1 << args.log2n
+    x, y = make_inputs(n, rank)
+    X = torch.from_numpy(x).cuda()
+    Y = torch.from_numpy(y).cuda()
+    Z = torch.zeros(2 * FOLD, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+    rb.call("rb_set_stream", stream.cuda_stream)
+
+    def step():
+        Z.zero_()
+        rb.call("binnedBLAS_dbddot", FOLD, n, X, 1, Y, 1, Z)
+
+    gathered = None
+    if world > 1:
+        gathered = torch.empty(world * 2 * FOLD, dtype=torch.float64, device="cuda")
+
+    def combine():
+        # exchange the 48-byte per-rank states and merge them on every GPU
+        dist.all_gather_into_tensor(gathered, Z)
+        total = torch.zeros(2 * FOLD, dtype=torch.float64, device="cuda")
+        rb.call("rb_dbdbadd_states", FOLD, world, gathered, total)
+        return total
+
+    for _ in range(args.warmup):
+        step()
+        if world > 1:
+            combine()
+    torch.cuda.synchronize()
+    launches0 = rb.lib.rb_kernel_launch_count()
+    clocks = ClockSampler(local_rank)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for i in range(args.steps):
+        ev[i][0].record(stream)
+        step()
+        ev[i][1].record(stream)
+        if world > 1:
+            combine()
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = rb.lib.rb_kernel_launch_count() - launches0
+    total_ms = t_start.elapsed_time(t_end)
+    kern_ms = [a.elapsed_time(b) for a, b in ev]
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = 16.0 * n * world / (ms_per_step * 1e-3) / 1e9
+    kernel_mean_ms = statistics.mean(kern_ms)
+    achieved = 16.0 * n / (kernel_mean_ms * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+
+    # result parity: the GPU state equals the reference CPU state (checked below on rank 0)
+    gpu_state = Z.cpu().numpy().copy()
+
+    # e2e: reference-facing call with pinned host buffers
+    xp = torch.from_numpy(x).pin_memory()
+    yp = torch.from_numpy(y).pin_memory()
+    e2e_val = None
+    e2e_ms = None
+    res = None
+    if args.e2e_steps > 0:
+        res = rb.call("reproBLAS_rddot", FOLD, n, xp, 1, yp, 1)   # warm the staging ring
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            res = rb.call("reproBLAS_rddot", FOLD, n, xp, 1, yp, 1)
+        t1 = time.perf_counter()
+        e2e_ms = (t1 - t0) * 1e3 / args.e2e_steps
+        if world > 1:
+            t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        e2e_val = 16.0 * n * world / (e2e_ms * 1e-3) / 1e9
+
+    cpu = None
+    bit_identical = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from _ffi import ref, port
+        R = ref()
+        kind = "reference"
+        if R is None:
+            R = port()
+            kind = "port"
+        threads = host_threads()
+        cpu_reference_dot(R, x[: 1 << 20], y[: 1 << 20], threads)   # warm-up
+        times = []
+        state = None
+        for _ in range(3):
+            dt, state = cpu_reference_dot(R, x, y, threads)
+            times.append(dt)
+        cpu_gbs = 16.0 * n / min(times) / 1e9
+        bit_identical = bool(state.tobytes() == gpu_state.tobytes())
+        cpu = {"value": round(cpu_gbs, 3), "unit": "GB/s", "cores": threads, "kind": kind,
+               "sample": "full N=2^%d workload, %d threads (contiguous chunks + binned_dbdbadd), "
+                         "best of 3" % (args.log2n, threads),
+               "bit_identical_to_gpu": bit_identical}
+
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic uniform(-1,1), seed 2024+rank (host-generated)",
+        "config": {"workload": "reproBLAS_ddot fold 3, N=2^%d FP64 per GPU (binnedBLAS_dbddot, "
+                               "device-resident inputs)" % args.log2n,
+                   "n_per_gpu": n, "fold": FOLD, "l2": "inputs 4 GiB >> 126 MB L2, no flush",
+                   "parallelism": "weak: shard per GPU, NCCL all-gather of 48-byte states"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                     "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                     "kernel": "rb::blas1_kernel<double,3,kOpDot,vec>",
+                     "kernel_ms": round(kernel_mean_ms, 5)},
+        "clocks": clk,
+        "gpu_launches": int(launches),
+        "e2e": {"value": round(e2e_val, 3) if e2e_val else None, "unit": "GB/s",
+                "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 8,
+                "ms_per_step": round(e2e_ms, 3) if e2e_ms else None,
+                "api": "reproBLAS_rddot(3, N, pinned host X, 1, pinned host Y, 1)"},
+        "cpu_baseline": cpu,
+        "result": res,
+    }
+    traffic = os.path.join(ROOT, "profiles", "ddot_traffic.json")
+    if os.path.exists(traffic):
+        try:
+            with open(traffic) as f:
+                line["roofline"]["traffic"] = json.load(f)["bytes_per_launch_at_2^28"]
+        except Exception:
+            pass
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+    else:
+        ours_arm(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,174 @@
+/*
+ * reproblas_b200.h -- C ABI of the B200 (sm_100a) reproducible binned BLAS.
+ *
+ * A drop-in for ReproBLAS v2.1.0's reproBLAS_* and binnedBLAS_* entry points on the
+ * binned-accumulation hot path. Every function keeps the reference's name, argument list
+ * and meaning (fold, Order/Trans characters, strides, accumulate-into-caller semantics) and
+ * returns results bit-identical to the reference CPU library on the same inputs and fold.
+ * Binned accumulators use the reference memory layout (include/binned.h:46-73):
+ *   double_binned of fold k:            [pri_0..pri_{k-1}, car_0..car_{k-1}]
+ *   double_complex_binned of fold k:    [pri re/im interleaved (2k), car re/im interleaved (2k)]
+ *   float_binned / float_complex_binned: the same with float
+ * so a GPU-produced accumulator can be merged on the host by the reference's
+ * binned_dbdbadd / binnedMPI_DBDBADD unchanged. Link this library in place of the
+ * reference's libreproblas and libbinnedblas; keep the reference's libbinned for host-side
+ * binned helpers (alloc, conv, merge).
+ *
+ * Pointers: every array argument (vectors, matrices, binned accumulators, complex results)
+ * may point to device memory (cudaMalloc / managed) or to host memory (pinned or pageable).
+ * Host inputs are staged to the GPU in chunks that overlap the copies with the kernels;
+ * host outputs are copied back before the call returns.
+ *
+ * Streams: work is issued on the calling thread's current stream (rb_set_stream; default
+ * the legacy default stream). Calls that return a value, or that write host memory,
+ * synchronise that stream before returning. binnedBLAS_* calls whose accumulator and
+ * inputs are all in device memory only enqueue work.
+ *
+ * Errors: the reference has no error returns. Here invalid arguments (fold outside 2..8,
+ * negative strides, misaligned element pointers) and CUDA failures set a thread-local error
+ * (rb_get_last_error); value-returning functions then return NaN and others leave their
+ * outputs untouched. N <= 0 behaves as in the reference (nothing is deposited).
+ *
+ * Supported folds: 2..8 (the reference default is 3, DIDEFAULTFOLD / SIDEFAULTFOLD).
+ */
+#ifndef REPROBLAS_B200_H
+#define REPROBLAS_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef double double_binned;          /* include/binned.h:46 */
+typedef double double_complex_binned;  /* include/binned.h:55 */
+typedef float float_binned;            /* include/binned.h:64 */
+typedef float float_complex_binned;    /* include/binned.h:73 */
+
+/* ------------------------------------------------------------------------------------
+ * reproBLAS level (value-returning; temporaries are internal). include/reproBLAS.h
+ * ------------------------------------------------------------------------------------ */
+
+/* include/reproBLAS.h:27 (src/reproBLAS/rdsum.c:20-31) */
+double reproBLAS_rdsum(const int fold, const int N, const double *X, const int incX);
+/* include/reproBLAS.h:97 (src/reproBLAS/dsum.c:20), fold 3 */
+double reproBLAS_dsum(const int N, const double *X, const int incX);
+
+/* include/reproBLAS.h:30 (src/reproBLAS/rddot.c:22-33) */
+double reproBLAS_rddot(const int fold, const int N, const double *X, const int incX,
+                       const double *Y, const int incY);
+/* include/reproBLAS.h:100 (src/reproBLAS/ddot.c:22), fold 3 */
+double reproBLAS_ddot(const int N, const double *X, const int incX, const double *Y,
+                      const int incY);
+
+/* include/reproBLAS.h:29 (src/reproBLAS/rdnrm2.c:22-34) */
+double reproBLAS_rdnrm2(const int fold, const int N, const double *X, const int incX);
+/* include/reproBLAS.h:99 (src/reproBLAS/dnrm2.c:20), fold 3 */
+double reproBLAS_dnrm2(const int N, const double *X, const int incX);
+
+/* include/reproBLAS.h:34 (src/reproBLAS/rssum.c:20-31) */
+float reproBLAS_rssum(const int fold, const int N, const float *X, const int incX);
+/* include/reproBLAS.h:104 (src/reproBLAS/ssum.c), fold 3 */
+float reproBLAS_ssum(const int N, const float *X, const int incX);
+
+/* include/reproBLAS.h:32 (src/reproBLAS/rsdot.c:22-33) */
+float reproBLAS_rsdot(const int fold, const int N, const float *X, const int incX,
+                      const float *Y, const int incY);
+/* include/reproBLAS.h:102 (src/reproBLAS/sdot.c), fold 3 */
+float reproBLAS_sdot(const int N, const float *X, const int incX, const float *Y,
+                     const int incY);
+
+/* include/reproBLAS.h:37 (src/reproBLAS/rzsum_sub.c:20-30): sum of complex128 into *sum;
+ * default fold: include/reproBLAS.h:107 */
+void reproBLAS_rzsum_sub(const int fold, const int N, const void *X, const int incX,
+                         void *sum);
+void reproBLAS_zsum_sub(const int N, const void *X, const int incX, void *sum);
+
+/* include/reproBLAS.h:40 (src/reproBLAS/rzdotc_sub.c:22-32): conj(X)^T Y into *dotc;
+ * default fold: include/reproBLAS.h:110 */
+void reproBLAS_rzdotc_sub(const int fold, const int N, const void *X, const int incX,
+                          const void *Y, const int incY, void *dotc);
+void reproBLAS_zdotc_sub(const int N, const void *X, const int incX, const void *Y,
+                         const int incY, void *dotc);
+
+/* include/reproBLAS.h:43 (src/reproBLAS/rcsum_sub.c:20-30): sum of complex64 into *sum;
+ * default fold: include/reproBLAS.h:113 */
+void reproBLAS_rcsum_sub(const int fold, const int N, const void *X, const int incX,
+                         void *sum);
+void reproBLAS_csum_sub(const int N, const void *X, const int incX, void *sum);
+
+/* ------------------------------------------------------------------------------------
+ * binnedBLAS level: add into a caller-owned binned accumulator (resumable state).
+ * include/binnedBLAS.h
+ * ------------------------------------------------------------------------------------ */
+
+/* include/binnedBLAS.h:47 (src/binnedBLAS/dbdsum.c:17 -> dmdsum.ccog:56-90) */
+void binnedBLAS_dbdsum(const int fold, const int N, const double *X, const int incX,
+                       double_binned *Y);
+/* include/binnedBLAS.h:53 (src/binnedBLAS/dbddot.c:19 -> dmddot.ccog:59-101) */
+void binnedBLAS_dbddot(const int fold, const int N, const double *X, const int incX,
+                       const double *Y, const int incY, double_binned *Z);
+/* include/binnedBLAS.h:51 (src/binnedBLAS/dbdssq.c:19 -> dmdssq.ccog:59-101): returns the
+ * new scale; the accumulator holds sum((x/scale)^2) */
+double binnedBLAS_dbdssq(const int fold, const int N, const double *X, const int incX,
+                         const double scaleY, double_binned *Y);
+/* include/binnedBLAS.h:67 (src/binnedBLAS/sbssum.c -> smssum.ccog) */
+void binnedBLAS_sbssum(const int fold, const int N, const float *X, const int incX,
+                       float_binned *Y);
+/* include/binnedBLAS.h:73 (src/binnedBLAS/sbsdot.c -> smsdot.ccog:59-100) */
+void binnedBLAS_sbsdot(const int fold, const int N, const float *X, const int incX,
+                       const float *Y, const int incY, float_binned *Z);
+/* include/binnedBLAS.h:56 (src/binnedBLAS/zbzsum.c:17 -> zmzsum.ccog:56-110) */
+void binnedBLAS_zbzsum(const int fold, const int N, const void *X, const int incX,
+                       double_complex_binned *Y);
+/* include/binnedBLAS.h:64 (src/binnedBLAS/zbzdotc.c:19 -> zmzdotc.ccog:58-120) */
+void binnedBLAS_zbzdotc(const int fold, const int N, const void *X, const int incX,
+                        const void *Y, const int incY, double_complex_binned *Z);
+/* include/binnedBLAS.h:76 (src/binnedBLAS/cbcsum.c -> cmcsum.ccog) */
+void binnedBLAS_cbcsum(const int fold, const int N, const void *X, const int incX,
+                       float_complex_binned *Y);
+
+/* ------------------------------------------------------------------------------------
+ * B200 controls (no reference counterpart)
+ * ------------------------------------------------------------------------------------ */
+
+/* Error codes of the thread-local error side channel. */
+enum {
+  RB_SUCCESS = 0,
+  RB_ERR_INVALID_ARG = 1,    /* fold outside 2..8, negative stride, bad Order/Trans, ... */
+  RB_ERR_CUDA = 2,           /* a CUDA runtime call failed (message has the details) */
+  RB_ERR_ALLOC = 3,          /* device or pinned allocation failed */
+  RB_ERR_UNSUPPORTED = 4     /* a valid request this build does not implement */
+};
+/* Last error raised on the calling thread (RB_SUCCESS if none since rb_clear_error). */
+int rb_get_last_error(void);
+/* Human-readable message of the last error on the calling thread. */
+const char *rb_get_last_error_message(void);
+void rb_clear_error(void);
+
+/* Stream for subsequent calls from the calling thread (a cudaStream_t; NULL = legacy
+ * default stream). */
+void rb_set_stream(void *stream);
+void *rb_get_stream(void);
+
+/* Launch-shape override for the reductions (process-wide): CTAs per SM, threads per CTA
+ * (a multiple of 32, at most 256). 0 selects the default. Results do not depend on it;
+ * it exists to demonstrate and test that. */
+void rb_set_launch_config(int ctas_per_sm, int threads_per_cta);
+
+/* Number of kernels this library launched since load (all threads). */
+unsigned long long rb_kernel_launch_count(void);
+
+/* out += states[0] + ... + states[count-1], all fold-`fold` double_binned in DEVICE
+ * memory, merged on the GPU with the reference's binned_dbdbadd arithmetic (the operation
+ * binnedMPI_DBDBADD applies, src/binnedMPI/DBDBADD.ccog:22-24). Enqueued on the current
+ * stream. Combines per-GPU partial states after an all-gather; any order gives the same
+ * bits. Returns an RB_* code. */
+int rb_dbdbadd_states(const int fold, const int count, const double_binned *states,
+                      double_binned *out);
+
+/* Library version string. */
+const char *rb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* REPROBLAS_B200_H */

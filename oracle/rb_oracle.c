@@ -1,0 +1,1019 @@
+/*
+ * rb_oracle.c -- CPU restatement of ReproBLAS v2.1.0's binned accumulation (scalar form).
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for the CUDA product, never part of it.
+ *
+ * Each routine restates the reference routine named in its comment (paths relative to the
+ * ReproBLAS source tree). The reference's vectorised deposit loops are generated code whose
+ * SIMD lanes are combined exactly (src/binned/deposit.py:267-326); the reference's own AVX
+ * and scalar builds are bit-identical, so the scalar form below defines the same bits.
+ * Parity of this file with the compiled reference is checked in tests/test_oracle_pin.py.
+ *
+ * Build: make -C oracle port   (plain C11, -ffp-contract=off, no fast-math).
+ */
+#include "rb_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------------- */
+/* Constants: include/binned.h:84-217                                          */
+/* ------------------------------------------------------------------------- */
+#define DBW 40                                   /* DBWIDTH, binned.h:84 */
+#define SBW 13                                   /* SBWIDTH, binned.h:95 */
+#define DMAXINDEX (((DBL_MAX_EXP - DBL_MIN_EXP + DBL_MANT_DIG - 1) / DBW) - 1)   /* 51 */
+#define DMAXFOLD (DMAXINDEX + 1)                                                /* 52 */
+#define SMAXINDEX (((FLT_MAX_EXP - FLT_MIN_EXP + FLT_MANT_DIG - 1) / SBW) - 1)  /* 20 */
+#define SMAXFOLD (SMAXINDEX + 1)                                                /* 21 */
+#define DENDURANCE (1 << (DBL_MANT_DIG - DBW - 2))                              /* 2048 */
+#define SENDURANCE (1 << (FLT_MANT_DIG - SBW - 2))                              /* 512 */
+#define DCOMPRESSION (1.0 / (1 << (DBL_MANT_DIG - DBW + 1)))                    /* 2^-14 */
+#define DEXPANSION (1.0 * (1 << (DBL_MANT_DIG - DBW + 1)))                      /* 2^14 */
+#define SCOMPRESSION (1.0 / (1 << (FLT_MANT_DIG - SBW + 1)))                    /* 2^-12 */
+#define SEXPANSION (1.0 * (1 << (FLT_MANT_DIG - SBW + 1)))                      /* 2^12 */
+#define DEXP_BIAS (DBL_MAX_EXP - 2)                                             /* common.h:56 */
+#define SEXP_BIAS (FLT_MAX_EXP - 2)                                             /* common.h:71 */
+
+/* Block lengths of the reference's block loops (N_block_MAX in each .ccog). */
+#define NB_DDOT 1024   /* src/binnedBLAS/dmddot.ccog:36 */
+#define NB_DSUM 2048   /* src/binnedBLAS/dmdsum.ccog:36 */
+#define NB_DSSQ 2048   /* src/binnedBLAS/dmdssq.ccog:36 */
+#define NB_ZSUM 2048   /* src/binnedBLAS/zmzsum.ccog:36 */
+#define NB_ZDOT 2048   /* src/binnedBLAS/zmzdotc.ccog:36 */
+#define NB_SSUM 512    /* src/binnedBLAS/smssum.ccog:37 */
+#define NB_SDOT 512    /* src/binnedBLAS/smsdot.ccog:36 */
+#define NB_CSUM 512    /* src/binnedBLAS/cmcsum.ccog:36 */
+
+static inline int imin(int a, int b) { return a < b ? a : b; }
+static inline int imax(int a, int b) { return a > b ? a : b; }
+
+/* Bit helpers: src/common/common.h:65-115 */
+static inline uint64_t dbits(double x) { uint64_t u; memcpy(&u, &x, 8); return u; }
+static inline double bitsd(uint64_t u) { double x; memcpy(&x, &u, 8); return x; }
+static inline uint32_t fbits(float x) { uint32_t u; memcpy(&u, &x, 4); return u; }
+static inline float bitsf(uint32_t u) { float x; memcpy(&x, &u, 4); return x; }
+static inline int dexp(double x) { return (int)((dbits(x) >> 52) & 0x7ff); }
+static inline int fexp(float x) { return (int)((fbits(x) >> 23) & 0xff); }
+static inline int dnonfinite(double x) { return dexp(x) == 0x7ff; }
+static inline int fnonfinite(float x) { return fexp(x) == 0xff; }
+/* q.l |= 1: the "round to odd" sticky bit of every deposit (dmddeposit.c:38,48,55) */
+static inline double dodd(double x) { return bitsd(dbits(x) | 1u); }
+static inline float fodd(float x) { return bitsf(fbits(x) | 1u); }
+
+/* ------------------------------------------------------------------------- */
+/* FP64 primitives                                                            */
+/* ------------------------------------------------------------------------- */
+
+/* Bin table: src/binned/dmbins.c:23-39. bins[0] = 1.5*2^1023, bins[i] = 0.75*2^(1038-40i),
+ * padded with bins[51] up to index 51+52. */
+static double g_dbins[DMAXINDEX + DMAXFOLD];
+static int g_dbins_ready = 0;
+const double *rbo_dmbins(int index) {
+  if (!g_dbins_ready) {
+    int i;
+    g_dbins[0] = 2.0 * ldexp(0.75, DBL_MAX_EXP - 1);
+    for (i = 1; i <= DMAXINDEX; i++)
+      g_dbins[i] = ldexp(0.75, DBL_MAX_EXP + DBL_MANT_DIG - DBW + 1 - i * DBW);
+    for (; i < DMAXINDEX + DMAXFOLD; i++) g_dbins[i] = g_dbins[i - 1];
+    g_dbins_ready = 1;
+  }
+  return g_dbins + index;
+}
+
+/* src/binned/dindex.c:19-41 */
+int rbo_dindex(double x) {
+  int e = dexp(x);
+  if (e == 0) {
+    if (x == 0.0) return DMAXINDEX;
+    int fe;
+    frexp(x, &fe);
+    return imin((DBL_MAX_EXP - fe) / DBW, DMAXINDEX);
+  }
+  return ((DBL_MAX_EXP + DEXP_BIAS) - e) / DBW;
+}
+
+/* src/binned/dmindex.c:22-38 */
+int rbo_dmindex(const double *pri) {
+  return ((DBL_MAX_EXP + DBL_MANT_DIG - DBW + 1 + DEXP_BIAS) - dexp(pri[0])) / DBW;
+}
+
+/* src/binned/dmindex0.c:19-31 */
+int rbo_dmindex0(const double *pri) { return dexp(pri[0]) == DBL_MAX_EXP + DEXP_BIAS; }
+
+/* src/binned/dmdupdate.c:24-56 */
+void rbo_dmdupdate(int fold, double x, double *pri, int incpri, double *car, int inccar) {
+  if (dnonfinite(pri[0])) return;
+  int xi = rbo_dindex(x);
+  if (pri[0] == 0.0) {
+    const double *b = rbo_dmbins(xi);
+    for (int i = 0; i < fold; i++) { pri[i * incpri] = b[i]; car[i * inccar] = 0.0; }
+    return;
+  }
+  int shift = rbo_dmindex(pri) - xi;
+  if (shift > 0) {
+    int i;
+    for (i = fold - 1; i >= shift; i--) {
+      pri[i * incpri] = pri[(i - shift) * incpri];
+      car[i * inccar] = car[(i - shift) * inccar];
+    }
+    const double *b = rbo_dmbins(xi);
+    for (int j = 0; j < i + 1; j++) { pri[j * incpri] = b[j]; car[j * inccar] = 0.0; }
+  }
+}
+
+/* src/binned/dmddeposit.c:24-71 */
+void rbo_dmddeposit(int fold, double x, double *pri, int incpri) {
+  if (dnonfinite(x) || dnonfinite(pri[0])) { pri[0] += x; return; }
+  int i = 0;
+  if (rbo_dmindex0(pri)) {
+    double M = pri[0];
+    double q = dodd(x * DCOMPRESSION);
+    q += M;
+    pri[0] = q;
+    M -= q;
+    M *= DEXPANSION * 0.5;
+    x += M;
+    x += M;
+    i = 1;
+  }
+  for (; i < fold - 1; i++) {
+    double M = pri[i * incpri];
+    double q = dodd(x) + M;
+    pri[i * incpri] = q;
+    x += M - q;
+  }
+  pri[i * incpri] += dodd(x);
+}
+
+/* src/binned/dmrenorm.c:70-86: move bits 50..51 of each primary into its carry. */
+void rbo_dmrenorm(int fold, double *pri, int incpri, double *car, int inccar) {
+  if (pri[0] == 0.0 || dnonfinite(pri[0])) return;
+  for (int i = 0; i < fold; i++) {
+    uint64_t u = dbits(pri[i * incpri]);
+    car[i * inccar] += (double)((int)((u >> (DBL_MANT_DIG - 3)) & 3) - 2);
+    u &= ~(1ull << (DBL_MANT_DIG - 3));
+    u |= 1ull << (DBL_MANT_DIG - 2);
+    pri[i * incpri] = bitsd(u);
+  }
+}
+
+/* src/binned/dmdmadd.c:27-74 */
+void rbo_dmdmadd(int fold, const double *priX, int incpriX, const double *carX, int inccarX,
+                 double *priY, int incpriY, double *carY, int inccarY) {
+  if (priX[0] == 0.0) return;
+  if (priY[0] == 0.0) {
+    for (int i = 0; i < fold; i++) {
+      priY[i * incpriY] = priX[i * incpriX];
+      carY[i * inccarY] = carX[i * inccarX];
+    }
+    return;
+  }
+  if (dnonfinite(priX[0]) || dnonfinite(priY[0])) { priY[0] += priX[0]; return; }
+  int xi = rbo_dmindex(priX), yi = rbo_dmindex(priY);
+  int shift = yi - xi;
+  if (shift > 0) {
+    const double *b = rbo_dmbins(yi);
+    for (int i = fold - 1; i >= shift; i--) {
+      priY[i * incpriY] = priX[i * incpriX] + (priY[(i - shift) * incpriY] - b[i - shift]);
+      carY[i * inccarY] = carX[i * inccarX] + carY[(i - shift) * inccarY];
+    }
+    for (int i = 0; i < shift && i < fold; i++) {
+      priY[i * incpriY] = priX[i * incpriX];
+      carY[i * inccarY] = carX[i * inccarX];
+    }
+  } else {
+    const double *b = rbo_dmbins(xi);
+    for (int i = -shift; i < fold; i++) {
+      priY[i * incpriY] += priX[(i + shift) * incpriX] - b[i + shift];
+      carY[i * inccarY] += carX[(i + shift) * inccarX];
+    }
+  }
+  rbo_dmrenorm(fold, priY, incpriY, carY, inccarY);
+}
+
+/* src/binned/dbdbadd.c:16-18 */
+void rbo_dbdbadd(int fold, const double *X, double *Y) {
+  rbo_dmdmadd(fold, X, 1, X + fold, 1, Y, 1, Y + fold, 1);
+}
+
+/* src/binned/dbdconv.c + dmdconv.c:18-21 + dmdadd.c:20-24 */
+void rbo_dbdconv(int fold, double x, double *Y) {
+  memset(Y, 0, 2 * (size_t)fold * sizeof(double));
+  rbo_dmdupdate(fold, x, Y, 1, Y + fold, 1);
+  rbo_dmddeposit(fold, x, Y, 1);
+  rbo_dmrenorm(fold, Y, 1, Y + fold, 1);
+}
+
+/* src/binned/ddmconv.c:23-81: fixed-order conversion with scaling near overflow. */
+double rbo_ddmconv(int fold, const double *pri, int incpri, const double *car, int inccar) {
+  if (dnonfinite(pri[0])) return pri[0];
+  if (pri[0] == 0.0) return 0.0;
+  double Y = 0.0;
+  int i = 0;
+  int X_index = rbo_dmindex(pri);
+  const double *b = rbo_dmbins(X_index);
+  if (X_index <= (3 * DBL_MANT_DIG) / DBW) {
+    double sd = ldexp(0.5, 1 - (2 * DBL_MANT_DIG - DBW));
+    double su = ldexp(0.5, 1 + (2 * DBL_MANT_DIG - DBW));
+    int scaled = imax(imin(fold, (3 * DBL_MANT_DIG) / DBW - X_index), 0);
+    if (X_index == 0) {
+      Y += car[0] * ((b[0] / 6.0) * sd * DEXPANSION);
+      Y += car[inccar] * ((b[1] / 6.0) * sd);
+      Y += (pri[0] - b[0]) * sd * DEXPANSION;
+      i = 2;
+    } else {
+      Y += car[0] * ((b[0] / 6.0) * sd);
+      i = 1;
+    }
+    for (; i < scaled; i++) {
+      Y += car[i * inccar] * ((b[i] / 6.0) * sd);
+      Y += (pri[(i - 1) * incpri] - b[i - 1]) * sd;
+    }
+    if (i == fold) {
+      Y += (pri[(fold - 1) * incpri] - b[fold - 1]) * sd;
+      return Y * su;
+    }
+    if (isinf(Y * su)) return Y * su;
+    Y *= su;
+    for (; i < fold; i++) {
+      Y += car[i * inccar] * (b[i] / 6.0);
+      Y += pri[(i - 1) * incpri] - b[i - 1];
+    }
+    Y += pri[(fold - 1) * incpri] - b[fold - 1];
+  } else {
+    Y += car[0] * (b[0] / 6.0);
+    for (i = 1; i < fold; i++) {
+      Y += car[i * inccar] * (b[i] / 6.0);
+      Y += pri[(i - 1) * incpri] - b[i - 1];
+    }
+    Y += pri[(fold - 1) * incpri] - b[fold - 1];
+  }
+  return Y;
+}
+
+double rbo_ddbconv(int fold, const double *X) { return rbo_ddmconv(fold, X, 1, X + fold, 1); }
+
+/* src/binned/dscale.c:25-31 */
+double rbo_dscale(double x) {
+  int e = dexp(x);
+  e = e < DBW ? DBW : e;
+  e -= (e - DEXP_BIAS - 1) % DBW;
+  e -= DEXP_BIAS;
+  return ldexp(0.5, e);
+}
+
+/* src/binned/dmdrescale.c:20-37 */
+void rbo_dmdrescale(int fold, double x, double scaleY, double *pri, int incpri, double *car,
+                    int inccar) {
+  if (x == scaleY || x == 0.0 || scaleY == 0.0) return;
+  double r = x / scaleY;
+  r *= r;
+  for (int i = 0; i < fold; i++) {
+    pri[i * incpri] /= r;
+    if (pri[i * incpri] == 0.0) {
+      rbo_dmdupdate(fold - i, 0.0, pri + i * incpri, incpri, car + i * inccar, inccar);
+      return;
+    }
+  }
+}
+
+/* src/binned/dmdmaddsq.c:26-41 + dbdbaddsq.c:19-21 */
+double rbo_dbdbaddsq(int fold, double scaleX, const double *X, double scaleY, double *Y) {
+  if (scaleX > scaleY) {
+    rbo_dmdrescale(fold, scaleX, scaleY, Y, 1, Y + fold, 1);
+    rbo_dbdbadd(fold, X, Y);
+    return scaleX;
+  } else if (scaleX == scaleY) {
+    rbo_dbdbadd(fold, X, Y);
+    return scaleX;
+  } else {
+    double tmp[2 * DMAXFOLD];
+    memcpy(tmp, X, 2 * (size_t)fold * sizeof(double));
+    rbo_dmdrescale(fold, scaleY, scaleX, tmp, 1, tmp + fold, 1);
+    rbo_dbdbadd(fold, tmp, Y);
+    return scaleY;
+  }
+}
+
+/* src/binned/dbbound.c:21-23 */
+double rbo_dbbound(int fold, int N, double X, double S) {
+  return fmax(fabs(X), ldexp(0.5, DBL_MIN_EXP - 1)) * ldexp(0.5, (1 - fold) * DBW + 1) * N +
+         ((7.0 * DBL_EPSILON) / (1.0 - 6.0 * sqrt(DBL_EPSILON) - 7.0 * DBL_EPSILON)) * fabs(S);
+}
+
+/* ------------------------------------------------------------------------- */
+/* FP32 primitives (src/binned/s*.c, same structure as FP64)                  */
+/* ------------------------------------------------------------------------- */
+
+/* src/binned/smbins.c:23-39 */
+static float g_sbins[SMAXINDEX + SMAXFOLD];
+static int g_sbins_ready = 0;
+const float *rbo_smbins(int index) {
+  if (!g_sbins_ready) {
+    int i;
+    g_sbins[0] = ldexpf(0.75f, FLT_MAX_EXP);
+    for (i = 1; i <= SMAXINDEX; i++)
+      g_sbins[i] = ldexpf(0.75f, FLT_MAX_EXP + FLT_MANT_DIG - SBW + 1 - i * SBW);
+    for (; i < SMAXINDEX + SMAXFOLD; i++) g_sbins[i] = g_sbins[i - 1];
+    g_sbins_ready = 1;
+  }
+  return g_sbins + index;
+}
+
+/* src/binned/sindex.c:19-41 */
+int rbo_sindex(float x) {
+  int e = fexp(x);
+  if (e == 0) {
+    if (x == 0.0f) return SMAXINDEX;
+    int fe;
+    frexpf(x, &fe);
+    return imin((FLT_MAX_EXP - fe) / SBW, SMAXINDEX);
+  }
+  return ((FLT_MAX_EXP + SEXP_BIAS) - e) / SBW;
+}
+
+/* src/binned/smindex.c:22-38 */
+int rbo_smindex(const float *pri) {
+  return ((FLT_MAX_EXP + FLT_MANT_DIG - SBW + 1 + SEXP_BIAS) - fexp(pri[0])) / SBW;
+}
+
+static int smindex0(const float *pri) { return fexp(pri[0]) == FLT_MAX_EXP + SEXP_BIAS; }
+
+/* src/binned/smsupdate.c:24-56 */
+void rbo_smsupdate(int fold, float x, float *pri, int incpri, float *car, int inccar) {
+  if (fnonfinite(pri[0])) return;
+  int xi = rbo_sindex(x);
+  if (pri[0] == 0.0f) {
+    const float *b = rbo_smbins(xi);
+    for (int i = 0; i < fold; i++) { pri[i * incpri] = b[i]; car[i * inccar] = 0.0f; }
+    return;
+  }
+  int shift = rbo_smindex(pri) - xi;
+  if (shift > 0) {
+    int i;
+    for (i = fold - 1; i >= shift; i--) {
+      pri[i * incpri] = pri[(i - shift) * incpri];
+      car[i * inccar] = car[(i - shift) * inccar];
+    }
+    const float *b = rbo_smbins(xi);
+    for (int j = 0; j < i + 1; j++) { pri[j * incpri] = b[j]; car[j * inccar] = 0.0f; }
+  }
+}
+
+/* src/binned/smsdeposit.c:24-71. The compression constants are doubles in C, so the
+ * scaled products are formed in double and rounded back to float (exact: powers of 2). */
+void rbo_smsdeposit(int fold, float x, float *pri, int incpri) {
+  if (fnonfinite(x) || fnonfinite(pri[0])) { pri[0] += x; return; }
+  int i = 0;
+  if (smindex0(pri)) {
+    float M = pri[0];
+    float q = fodd((float)(x * SCOMPRESSION));
+    q += M;
+    pri[0] = q;
+    M -= q;
+    M = (float)(M * (SEXPANSION * 0.5));
+    x += M;
+    x += M;
+    i = 1;
+  }
+  for (; i < fold - 1; i++) {
+    float M = pri[i * incpri];
+    float q = fodd(x) + M;
+    pri[i * incpri] = q;
+    x += M - q;
+  }
+  pri[i * incpri] += fodd(x);
+}
+
+/* src/binned/smrenorm.c:70-86 */
+void rbo_smrenorm(int fold, float *pri, int incpri, float *car, int inccar) {
+  if (pri[0] == 0.0f || fnonfinite(pri[0])) return;
+  for (int i = 0; i < fold; i++) {
+    uint32_t u = fbits(pri[i * incpri]);
+    car[i * inccar] += (float)((int)((u >> (FLT_MANT_DIG - 3)) & 3) - 2);
+    u &= ~(1u << (FLT_MANT_DIG - 3));
+    u |= 1u << (FLT_MANT_DIG - 2);
+    pri[i * incpri] = bitsf(u);
+  }
+}
+
+/* src/binned/smsmadd.c:27-74 */
+void rbo_smsmadd(int fold, const float *priX, int incpriX, const float *carX, int inccarX,
+                 float *priY, int incpriY, float *carY, int inccarY) {
+  if (priX[0] == 0.0f) return;
+  if (priY[0] == 0.0f) {
+    for (int i = 0; i < fold; i++) {
+      priY[i * incpriY] = priX[i * incpriX];
+      carY[i * inccarY] = carX[i * inccarX];
+    }
+    return;
+  }
+  if (fnonfinite(priX[0]) || fnonfinite(priY[0])) { priY[0] += priX[0]; return; }
+  int xi = rbo_smindex(priX), yi = rbo_smindex(priY);
+  int shift = yi - xi;
+  if (shift > 0) {
+    const float *b = rbo_smbins(yi);
+    for (int i = fold - 1; i >= shift; i--) {
+      priY[i * incpriY] = priX[i * incpriX] + (priY[(i - shift) * incpriY] - b[i - shift]);
+      carY[i * inccarY] = carX[i * inccarX] + carY[(i - shift) * inccarY];
+    }
+    for (int i = 0; i < shift && i < fold; i++) {
+      priY[i * incpriY] = priX[i * incpriX];
+      carY[i * inccarY] = carX[i * inccarX];
+    }
+  } else {
+    const float *b = rbo_smbins(xi);
+    for (int i = -shift; i < fold; i++) {
+      priY[i * incpriY] += priX[(i + shift) * incpriX] - b[i + shift];
+      carY[i * inccarY] += carX[(i + shift) * inccarX];
+    }
+  }
+  rbo_smrenorm(fold, priY, incpriY, carY, inccarY);
+}
+
+void rbo_sbsbadd(int fold, const float *X, float *Y) {
+  rbo_smsmadd(fold, X, 1, X + fold, 1, Y, 1, Y + fold, 1);
+}
+
+/* src/binned/ssmconv.c:22-57: accumulates in double in decreasing-exponent order. */
+float rbo_ssmconv(int fold, const float *pri, int incpri, const float *car, int inccar) {
+  if (fnonfinite(pri[0])) return pri[0];
+  if (pri[0] == 0.0f) return 0.0f;
+  double Y = 0.0;
+  int i;
+  int X_index = rbo_smindex(pri);
+  const float *b = rbo_smbins(X_index);
+  if (X_index == 0) {
+    Y += (double)car[0] * (double)(b[0] / 6.0) * (double)SEXPANSION;
+    Y += (double)car[inccar] * (double)(b[1] / 6.0);
+    Y += (double)(pri[0] - b[0]) * (double)SEXPANSION;
+    i = 2;
+  } else {
+    Y += (double)car[0] * (double)(b[0] / 6.0);
+    i = 1;
+  }
+  for (; i < fold; i++) {
+    Y += (double)car[i * inccar] * (double)(b[i] / 6.0);
+    Y += (double)(pri[(i - 1) * incpri] - b[i - 1]);
+  }
+  Y += (double)(pri[(fold - 1) * incpri] - b[fold - 1]);
+  return (float)Y;
+}
+
+float rbo_ssbconv(int fold, const float *X) { return rbo_ssmconv(fold, X, 1, X + fold, 1); }
+
+/* ------------------------------------------------------------------------- */
+/* Block loops (binnedBLAS)                                                    */
+/* ------------------------------------------------------------------------- */
+
+/* Scalar max of |v| as the reference's scalar amax loops write it (damax.ccog:282-306):
+ * m = (m > v ? m : v), so a NaN is kept only if it is the last element. */
+static inline double dmaxabs(double m, double v) { v = fabs(v); return m > v ? m : v; }
+static inline float smaxabs(float m, float v) { v = fabsf(v); return m > v ? m : v; }
+
+/* src/binnedBLAS/dmdsum.ccog:56-90 (via dbdsum.c:17) */
+void rbo_dbdsum(int fold, int N, const double *X, int incX, double *Y) {
+  double *pri = Y, *car = Y + fold;
+  int deposits = 0;
+  for (int i = 0; i < N; i += NB_DSUM) {
+    int nb = imin(N - i, NB_DSUM);
+    const double *x = X + (size_t)i * incX;
+    double amax = 0.0;
+    for (int j = 0; j < nb; j++) amax = dmaxabs(amax, x[(size_t)j * incX]);
+    if (isinf(amax) || isinf(pri[0]))
+      for (int j = 0; j < nb; j++) pri[0] += x[(size_t)j * incX];
+    if (isnan(pri[0])) return;
+    if (isinf(pri[0])) continue;
+    if (deposits + nb > DENDURANCE) { rbo_dmrenorm(fold, pri, 1, car, 1); deposits = 0; }
+    rbo_dmdupdate(fold, amax, pri, 1, car, 1);
+    for (int j = 0; j < nb; j++) rbo_dmddeposit(fold, x[(size_t)j * incX], pri, 1);
+    deposits += nb;
+  }
+  rbo_dmrenorm(fold, pri, 1, car, 1);
+}
+
+/* src/binnedBLAS/dmddot.ccog:59-101,12066-12072 (via dbddot.c:19) */
+void rbo_dbddot(int fold, int N, const double *X, int incX, const double *Y, int incY,
+                double *Z) {
+  double *pri = Z, *car = Z + fold;
+  int deposits = 0;
+  for (int i = 0; i < N; i += NB_DDOT) {
+    int nb = imin(N - i, NB_DDOT);
+    const double *x = X + (size_t)i * incX, *y = Y + (size_t)i * incY;
+    double amaxm = 0.0;
+    for (int j = 0; j < nb; j++) amaxm = dmaxabs(amaxm, x[(size_t)j * incX] * y[(size_t)j * incY]);
+    if (isinf(amaxm) || isinf(pri[0]))
+      for (int j = 0; j < nb; j++) pri[0] += x[(size_t)j * incX] * y[(size_t)j * incY];
+    if (isnan(pri[0])) return;
+    if (isinf(pri[0])) continue;
+    if (deposits + nb > DENDURANCE) { rbo_dmrenorm(fold, pri, 1, car, 1); deposits = 0; }
+    rbo_dmdupdate(fold, amaxm, pri, 1, car, 1);
+    for (int j = 0; j < nb; j++)
+      rbo_dmddeposit(fold, x[(size_t)j * incX] * y[(size_t)j * incY], pri, 1);
+    deposits += nb;
+  }
+  rbo_dmrenorm(fold, pri, 1, car, 1);
+}
+
+/* src/binnedBLAS/dmdssq.ccog:59-101,4960-4969 (via dbdssq.c:19): sum of (x/scl)^2 with a running
+ * power-of-two scale aligned to the bin width. Returns the scale. */
+double rbo_dbdssq(int fold, int N, const double *X, int incX, double scaleY, double *Y) {
+  double *pri = Y, *car = Y + fold;
+  double scl = scaleY;
+  int deposits = 0;
+  for (int i = 0; i < N; i += NB_DSSQ) {
+    int nb = imin(N - i, NB_DSSQ);
+    const double *x = X + (size_t)i * incX;
+    double amax = 0.0;
+    for (int j = 0; j < nb; j++) amax = dmaxabs(amax, x[(size_t)j * incX]);
+    if (isinf(amax) || isinf(pri[0]))
+      for (int j = 0; j < nb; j++) pri[0] += fabs(x[(size_t)j * incX]);
+    if (isnan(pri[0])) return rbo_dscale(1.0);
+    if (isinf(pri[0])) continue;
+    if (deposits + nb > DENDURANCE) { rbo_dmrenorm(fold, pri, 1, car, 1); deposits = 0; }
+    double nscl = rbo_dscale(amax);
+    if (nscl > scl) {
+      if (scl > 0.0) rbo_dmdrescale(fold, nscl, scl, pri, 1, car, 1);
+      scl = nscl;
+    }
+    amax /= scl;
+    amax = amax * amax;
+    rbo_dmdupdate(fold, amax, pri, 1, car, 1);
+    double inv = 1.0 / scl;   /* depositSSq.py:17: x * (1/scale), then squared */
+    for (int j = 0; j < nb; j++) {
+      double v = x[(size_t)j * incX] * inv;
+      rbo_dmddeposit(fold, v * v, pri, 1);
+    }
+    deposits += nb;
+  }
+  rbo_dmrenorm(fold, pri, 1, car, 1);
+  return dnonfinite(pri[0]) ? rbo_dscale(1.0) : scl;   /* dmdssq.ccog:4963-4969 */
+}
+
+/* src/binnedBLAS/smssum.ccog (via sbssum.c:17) */
+void rbo_sbssum(int fold, int N, const float *X, int incX, float *Y) {
+  float *pri = Y, *car = Y + fold;
+  int deposits = 0;
+  for (int i = 0; i < N; i += NB_SSUM) {
+    int nb = imin(N - i, NB_SSUM);
+    const float *x = X + (size_t)i * incX;
+    float amax = 0.0f;
+    for (int j = 0; j < nb; j++) amax = smaxabs(amax, x[(size_t)j * incX]);
+    if (isinf(amax) || isinf(pri[0]))
+      for (int j = 0; j < nb; j++) pri[0] += x[(size_t)j * incX];
+    if (isnan(pri[0])) return;
+    if (isinf(pri[0])) continue;
+    if (deposits + nb > SENDURANCE) { rbo_smrenorm(fold, pri, 1, car, 1); deposits = 0; }
+    rbo_smsupdate(fold, amax, pri, 1, car, 1);
+    for (int j = 0; j < nb; j++) rbo_smsdeposit(fold, x[(size_t)j * incX], pri, 1);
+    deposits += nb;
+  }
+  rbo_smrenorm(fold, pri, 1, car, 1);
+}
+
+/* src/binnedBLAS/smsdot.ccog:59-100 (via sbsdot.c) */
+void rbo_sbsdot(int fold, int N, const float *X, int incX, const float *Y, int incY, float *Z) {
+  float *pri = Z, *car = Z + fold;
+  int deposits = 0;
+  for (int i = 0; i < N; i += NB_SDOT) {
+    int nb = imin(N - i, NB_SDOT);
+    const float *x = X + (size_t)i * incX, *y = Y + (size_t)i * incY;
+    float amaxm = 0.0f;
+    for (int j = 0; j < nb; j++) amaxm = smaxabs(amaxm, x[(size_t)j * incX] * y[(size_t)j * incY]);
+    if (isinf(amaxm) || isinf(pri[0]))
+      for (int j = 0; j < nb; j++) pri[0] += x[(size_t)j * incX] * y[(size_t)j * incY];
+    if (isnan(pri[0])) return;
+    if (isinf(pri[0])) continue;
+    if (deposits + nb > SENDURANCE) { rbo_smrenorm(fold, pri, 1, car, 1); deposits = 0; }
+    rbo_smsupdate(fold, amaxm, pri, 1, car, 1);
+    for (int j = 0; j < nb; j++)
+      rbo_smsdeposit(fold, x[(size_t)j * incX] * y[(size_t)j * incY], pri, 1);
+    deposits += nb;
+  }
+  rbo_smrenorm(fold, pri, 1, car, 1);
+}
+
+/* Complex deposit of one element pair into the interleaved layout. The reference's
+ * generated complex loops deposit the two components independently, with the index-0
+ * compression chosen per component (zmzsum.ccog:6916-6990); a non-finite primary keeps
+ * receiving plain adds through the same chain, as the generated loop does. */
+static void zdeposit_component(int fold, double x, double *pri /* stride 2 */) {
+  int i = 0;
+  if (rbo_dmindex0(pri)) {
+    double M = pri[0];
+    double q = dodd(x * DCOMPRESSION) + M;
+    pri[0] = q;
+    M = (M - q) * (DEXPANSION * 0.5);
+    x = (x + M) + M;
+    i = 1;
+  }
+  for (; i < fold - 1; i++) {
+    double M = pri[2 * i];
+    double q = dodd(x) + M;
+    pri[2 * i] = q;
+    x += M - q;
+  }
+  pri[2 * i] += dodd(x);
+}
+
+static void zrenorm(int fold, double *Y) {
+  rbo_dmrenorm(fold, Y, 2, Y + 2 * fold, 2);
+  rbo_dmrenorm(fold, Y + 1, 2, Y + 2 * fold + 1, 2);
+}
+
+/* src/binnedBLAS/zmzsum.ccog:56-110 (via zbzsum.c:17) */
+void rbo_zbzsum(int fold, int N, const void *Xv, int incX, double *Y) {
+  const double *X = (const double *)Xv;
+  double *pri = Y, *car = Y + 2 * fold;
+  int deposits = 0;
+  for (int i = 0; i < N; i += NB_ZSUM) {
+    int nb = imin(N - i, NB_ZSUM);
+    const double *x = X + 2 * (size_t)i * incX;
+    double amax[2] = {0.0, 0.0};
+    for (int j = 0; j < nb; j++) {
+      amax[0] = dmaxabs(amax[0], x[2 * (size_t)j * incX]);
+      amax[1] = dmaxabs(amax[1], x[2 * (size_t)j * incX + 1]);
+    }
+    if (isinf(amax[0]) || isinf(pri[0]))
+      for (int j = 0; j < nb; j++) pri[0] += x[2 * (size_t)j * incX];
+    if (isinf(amax[1]) || isinf(pri[1]))
+      for (int j = 0; j < nb; j++) pri[1] += x[2 * (size_t)j * incX + 1];
+    if (isnan(pri[0]) && isnan(pri[1])) return;
+    if (isinf(pri[0]) && isinf(pri[1])) continue;
+    if (dnonfinite(pri[0])) amax[0] = pri[0];
+    if (dnonfinite(pri[1])) amax[1] = pri[1];
+    if (deposits + nb > DENDURANCE) { zrenorm(fold, Y); deposits = 0; }
+    rbo_dmdupdate(fold, amax[0], pri, 2, car, 2);       /* zmzupdate.c:20-23 */
+    rbo_dmdupdate(fold, amax[1], pri + 1, 2, car + 1, 2);
+    for (int j = 0; j < nb; j++) {
+      zdeposit_component(fold, x[2 * (size_t)j * incX], pri);
+      zdeposit_component(fold, x[2 * (size_t)j * incX + 1], pri + 1);
+    }
+    /* an infinite component is restored after the deposits (zmzsum.ccog:7028-7033) */
+    if (isinf(amax[0])) pri[0] = amax[0];
+    if (isinf(amax[1])) pri[1] = amax[1];
+    deposits += nb;
+  }
+  zrenorm(fold, Y);
+}
+
+/* src/binnedBLAS/zmzdotc.ccog:58-120 (via zbzdotc.c:19): conj(x)*y. The real part
+ * receives fl(xr*yr) and fl(xi*yi); the imaginary part fl(xr*yi) and -fl(xi*yr), each
+ * deposited separately (depositDotC.py:14-23), hence the halved endurance. */
+void rbo_zbzdotc(int fold, int N, const void *Xv, int incX, const void *Yv, int incY,
+                 double *Z) {
+  const double *X = (const double *)Xv, *Yp = (const double *)Yv;
+  double *pri = Z, *car = Z + 2 * fold;
+  int deposits = 0;
+  for (int i = 0; i < N; i += NB_ZDOT) {
+    int nb = imin(N - i, NB_ZDOT);
+    const double *x = X + 2 * (size_t)i * incX, *y = Yp + 2 * (size_t)i * incY;
+    double amaxm[2] = {0.0, 0.0};
+    /* zamaxm_sub (amaxm.py:33-45): re over |xr*yr|,|xi*yi|; im over |xi*yi... */
+    for (int j = 0; j < nb; j++) {
+      double xr = x[2 * (size_t)j * incX], xi = x[2 * (size_t)j * incX + 1];
+      double yr = y[2 * (size_t)j * incY], yi = y[2 * (size_t)j * incY + 1];
+      amaxm[0] = dmaxabs(amaxm[0], xr * yr);
+      amaxm[1] = dmaxabs(amaxm[1], xi * yr);
+      amaxm[0] = dmaxabs(amaxm[0], xi * yi);
+      amaxm[1] = dmaxabs(amaxm[1], xr * yi);
+    }
+    if (isinf(amaxm[0]) || isinf(pri[0]))
+      for (int j = 0; j < nb; j++)
+        pri[0] += x[2 * (size_t)j * incX] * y[2 * (size_t)j * incY] +
+                  x[2 * (size_t)j * incX + 1] * y[2 * (size_t)j * incY + 1];
+    if (isinf(amaxm[1]) || isinf(pri[1]))
+      for (int j = 0; j < nb; j++)
+        pri[1] += x[2 * (size_t)j * incX] * y[2 * (size_t)j * incY + 1] -
+                  x[2 * (size_t)j * incX + 1] * y[2 * (size_t)j * incY];
+    if (isnan(pri[0]) && isnan(pri[1])) return;
+    if (isinf(pri[0]) && isinf(pri[1])) continue;
+    if (dnonfinite(pri[0])) amaxm[0] = pri[0];
+    if (dnonfinite(pri[1])) amaxm[1] = pri[1];
+    if (deposits + nb > DENDURANCE / 2) { zrenorm(fold, Z); deposits = 0; }
+    rbo_dmdupdate(fold, amaxm[0], pri, 2, car, 2);
+    rbo_dmdupdate(fold, amaxm[1], pri + 1, 2, car + 1, 2);
+    for (int j = 0; j < nb; j++) {
+      double xr = x[2 * (size_t)j * incX], xi = x[2 * (size_t)j * incX + 1];
+      double yr = y[2 * (size_t)j * incY], yi = y[2 * (size_t)j * incY + 1];
+      zdeposit_component(fold, xr * yr, pri);
+      zdeposit_component(fold, -(xi * yr), pri + 1);
+      zdeposit_component(fold, xi * yi, pri);
+      zdeposit_component(fold, xr * yi, pri + 1);
+    }
+    if (isinf(amaxm[0])) pri[0] = amaxm[0];   /* zmzdotc.ccog:10146-10151 */
+    if (isinf(amaxm[1])) pri[1] = amaxm[1];
+    deposits += nb;
+  }
+  zrenorm(fold, Z);
+}
+
+/* Float complex sum: src/binnedBLAS/cmcsum.ccog (via cbcsum.c), same structure as zmzsum. */
+static void cdeposit_component(int fold, float x, float *pri /* stride 2 */) {
+  int i = 0;
+  if (smindex0(pri)) {
+    float M = pri[0];
+    float q = fodd((float)(x * SCOMPRESSION)) + M;
+    pri[0] = q;
+    M = (float)((M - q) * (SEXPANSION * 0.5));
+    x = (x + M) + M;
+    i = 1;
+  }
+  for (; i < fold - 1; i++) {
+    float M = pri[2 * i];
+    float q = fodd(x) + M;
+    pri[2 * i] = q;
+    x += M - q;
+  }
+  pri[2 * i] += fodd(x);
+}
+
+static void crenorm(int fold, float *Y) {
+  rbo_smrenorm(fold, Y, 2, Y + 2 * fold, 2);
+  rbo_smrenorm(fold, Y + 1, 2, Y + 2 * fold + 1, 2);
+}
+
+void rbo_cbcsum(int fold, int N, const void *Xv, int incX, float *Y) {
+  const float *X = (const float *)Xv;
+  float *pri = Y, *car = Y + 2 * fold;
+  int deposits = 0;
+  for (int i = 0; i < N; i += NB_CSUM) {
+    int nb = imin(N - i, NB_CSUM);
+    const float *x = X + 2 * (size_t)i * incX;
+    float amax[2] = {0.0f, 0.0f};
+    for (int j = 0; j < nb; j++) {
+      amax[0] = smaxabs(amax[0], x[2 * (size_t)j * incX]);
+      amax[1] = smaxabs(amax[1], x[2 * (size_t)j * incX + 1]);
+    }
+    if (isinf(amax[0]) || isinf(pri[0]))
+      for (int j = 0; j < nb; j++) pri[0] += x[2 * (size_t)j * incX];
+    if (isinf(amax[1]) || isinf(pri[1]))
+      for (int j = 0; j < nb; j++) pri[1] += x[2 * (size_t)j * incX + 1];
+    if (isnan(pri[0]) && isnan(pri[1])) return;
+    if (isinf(pri[0]) && isinf(pri[1])) continue;
+    if (fnonfinite(pri[0])) amax[0] = pri[0];
+    if (fnonfinite(pri[1])) amax[1] = pri[1];
+    if (deposits + nb > SENDURANCE) { crenorm(fold, Y); deposits = 0; }
+    rbo_smsupdate(fold, amax[0], pri, 2, car, 2);
+    rbo_smsupdate(fold, amax[1], pri + 1, 2, car + 1, 2);
+    for (int j = 0; j < nb; j++) {
+      cdeposit_component(fold, x[2 * (size_t)j * incX], pri);
+      cdeposit_component(fold, x[2 * (size_t)j * incX + 1], pri + 1);
+    }
+    if (isinf(amax[0])) pri[0] = amax[0];     /* cmcsum.ccog:6397-6402 */
+    if (isinf(amax[1])) pri[1] = amax[1];
+    deposits += nb;
+  }
+  crenorm(fold, Y);
+}
+
+/* ------------------------------------------------------------------------- */
+/* BLAS2/3: src/binnedBLAS/dbdgemv.ccog:57-162, dbdgemm.ccog:61-420            */
+/* ------------------------------------------------------------------------- */
+static int is_row_major(char o) { return o == 'r' || o == 'R'; }
+static int is_notrans(char t) { return t == 'n' || t == 'N'; }
+
+/* Each output entry is a binned dot over the whole reduction dimension: the reference's
+ * blocking (X_BLOCK/XT_BLOCK chunks of dbddot into the same accumulator) yields the same
+ * binned state because the state depends only on the multiset of deposited products.
+ * alpha scales x (dbdgemv.ccog:86-95,110-119); column-major maps to row-major with the
+ * transpose flipped (dbdgemv.ccog:146-158). */
+void rbo_dbdgemv(int fold, char Order, char TransA, int M, int N, double alpha,
+                 const double *A, int lda, const double *X, int incX, double *Y, int incY) {
+  if (M == 0 || N == 0 || alpha == 0.0) return;
+  if (!is_row_major(Order)) {
+    rbo_dbdgemv(fold, 'r', is_notrans(TransA) ? 't' : 'n', N, M, alpha, A, lda, X, incX, Y, incY);
+    return;
+  }
+  int nt = is_notrans(TransA);
+  int lenx = nt ? N : M, leny = nt ? M : N;
+  double *bx = (double *)malloc((size_t)lenx * sizeof(double));
+  double *col = (double *)malloc((size_t)lenx * sizeof(double));
+  for (int j = 0; j < lenx; j++) bx[j] = alpha == 1.0 ? X[(size_t)j * incX] : X[(size_t)j * incX] * alpha;
+  for (int i = 0; i < leny; i++) {
+    double *acc = Y + (size_t)i * incY * 2 * fold;
+    if (nt) {
+      rbo_dbddot(fold, N, A + (size_t)i * lda, 1, bx, 1, acc);
+    } else {
+      for (int j = 0; j < M; j++) col[j] = A[(size_t)j * lda + i];
+      rbo_dbddot(fold, M, col, 1, bx, 1, acc);
+    }
+  }
+  free(col);
+  free(bx);
+}
+
+/* alpha scales A in every branch (dbdgemm.ccog:92-103,187,234,289,336,365-371);
+ * C_ij accumulates the products fl(fl(alpha*A_ik) * B_kj). */
+void rbo_dbdgemm(int fold, char Order, char TransA, char TransB, int M, int N, int K,
+                 double alpha, const double *A, int lda, const double *B, int ldb, double *C,
+                 int ldc) {
+  if (M == 0 || N == 0 || K == 0 || alpha == 0.0) return;
+  int row = is_row_major(Order);
+  int ta = !is_notrans(TransA), tb = !is_notrans(TransB);
+  double *arow = (double *)malloc((size_t)K * sizeof(double));
+  double *bcol = (double *)malloc((size_t)K * sizeof(double));
+  for (int i = 0; i < M; i++) {
+    for (int k = 0; k < K; k++) {
+      double a;
+      if (row) a = ta ? A[(size_t)k * lda + i] : A[(size_t)i * lda + k];
+      else     a = ta ? A[(size_t)i * lda + k] : A[(size_t)k * lda + i];
+      arow[k] = alpha == 1.0 ? a : a * alpha;
+    }
+    for (int j = 0; j < N; j++) {
+      for (int k = 0; k < K; k++) {
+        if (row) bcol[k] = tb ? B[(size_t)j * ldb + k] : B[(size_t)k * ldb + j];
+        else     bcol[k] = tb ? B[(size_t)k * ldb + j] : B[(size_t)j * ldb + k];
+      }
+      double *acc = row ? C + ((size_t)i * ldc + j) * 2 * fold : C + ((size_t)j * ldc + i) * 2 * fold;
+      rbo_dbddot(fold, K, arow, 1, bcol, 1, acc);
+    }
+  }
+  free(bcol);
+  free(arow);
+}
+
+/* ------------------------------------------------------------------------- */
+/* reproBLAS wrappers: src/reproBLAS/r*.c                                      */
+/* ------------------------------------------------------------------------- */
+double rbo_rdsum(int fold, int N, const double *X, int incX) {   /* rdsum.c:20-31 */
+  double acc[2 * DMAXFOLD] = {0};
+  rbo_dbdsum(fold, N, X, incX, acc);
+  return rbo_ddbconv(fold, acc);
+}
+
+double rbo_rddot(int fold, int N, const double *X, int incX, const double *Y, int incY) {
+  double acc[2 * DMAXFOLD] = {0};                                  /* rddot.c:22-33 */
+  rbo_dbddot(fold, N, X, incX, Y, incY, acc);
+  return rbo_ddbconv(fold, acc);
+}
+
+double rbo_rdnrm2(int fold, int N, const double *X, int incX) {  /* rdnrm2.c:22-34 */
+  double acc[2 * DMAXFOLD] = {0};
+  double scl = rbo_dbdssq(fold, N, X, incX, 0.0, acc);
+  return scl * sqrt(rbo_ddbconv(fold, acc));
+}
+
+float rbo_rssum(int fold, int N, const float *X, int incX) {     /* rssum.c:20-31 */
+  float acc[2 * SMAXFOLD] = {0};
+  rbo_sbssum(fold, N, X, incX, acc);
+  return rbo_ssbconv(fold, acc);
+}
+
+float rbo_rsdot(int fold, int N, const float *X, int incX, const float *Y, int incY) {
+  float acc[2 * SMAXFOLD] = {0};                                   /* rsdot.c:22-33 */
+  rbo_sbsdot(fold, N, X, incX, Y, incY, acc);
+  return rbo_ssbconv(fold, acc);
+}
+
+/* zzmconv_sub.c:18-21: each component converted with its own stride-2 view */
+static void zconv(int fold, const double *Y, double *out) {
+  out[0] = rbo_ddmconv(fold, Y, 2, Y + 2 * fold, 2);
+  out[1] = rbo_ddmconv(fold, Y + 1, 2, Y + 2 * fold + 1, 2);
+}
+
+void rbo_rzsum_sub(int fold, int N, const void *X, int incX, void *sum) {  /* rzsum_sub.c */
+  double acc[4 * DMAXFOLD] = {0};
+  rbo_zbzsum(fold, N, X, incX, acc);
+  zconv(fold, acc, (double *)sum);
+}
+
+void rbo_rzdotc_sub(int fold, int N, const void *X, int incX, const void *Y, int incY,
+                    void *dotc) {                                  /* rzdotc_sub.c:22-32 */
+  double acc[4 * DMAXFOLD] = {0};
+  rbo_zbzdotc(fold, N, X, incX, Y, incY, acc);
+  zconv(fold, acc, (double *)dotc);
+}
+
+void rbo_rcsum_sub(int fold, int N, const void *X, int incX, void *sum) {  /* rcsum_sub.c */
+  float acc[4 * SMAXFOLD] = {0};
+  rbo_cbcsum(fold, N, X, incX, acc);
+  ((float *)sum)[0] = rbo_ssmconv(fold, acc, 2, acc + 2 * fold, 2);
+  ((float *)sum)[1] = rbo_ssmconv(fold, acc + 1, 2, acc + 2 * fold + 1, 2);
+}
+
+/* rdgemv.c:35-87: y <- conv(binned(beta*y) + sum_j A_ij*(alpha*x_j)) */
+void rbo_rdgemv(int fold, char Order, char TransA, int M, int N, double alpha, const double *A,
+                int lda, const double *X, int incX, double beta, double *Y, int incY) {
+  if (N == 0 || M == 0) return;
+  int leny = is_notrans(TransA) ? M : N;
+  size_t nb = 2 * (size_t)fold;
+  double *YI = (double *)calloc((size_t)leny * nb, sizeof(double));
+  if (beta != 0.0)
+    for (int i = 0; i < leny; i++)
+      rbo_dbdconv(fold, beta == 1.0 ? Y[(size_t)i * incY] : Y[(size_t)i * incY] * beta, YI + i * nb);
+  rbo_dbdgemv(fold, Order, TransA, M, N, alpha, A, lda, X, incX, YI, 1);
+  for (int i = 0; i < leny; i++) Y[(size_t)i * incY] = rbo_ddbconv(fold, YI + i * nb);
+  free(YI);
+}
+
+/* rdgemm.c:41-105 */
+void rbo_rdgemm(int fold, char Order, char TransA, char TransB, int M, int N, int K,
+                double alpha, const double *A, int lda, const double *B, int ldb, double beta,
+                double *C, int ldc) {
+  if (M == 0 || N == 0) return;
+  int row = is_row_major(Order);
+  size_t nb = 2 * (size_t)fold;
+  double *CI = (double *)calloc((size_t)M * N * nb, sizeof(double));
+  int ldci = row ? N : M;
+  for (int i = 0; i < M; i++)
+    for (int j = 0; j < N; j++) {
+      size_t c = row ? (size_t)i * ldc + j : (size_t)j * ldc + i;
+      size_t ci = row ? (size_t)i * ldci + j : (size_t)j * ldci + i;
+      if (beta != 0.0) rbo_dbdconv(fold, beta == 1.0 ? C[c] : C[c] * beta, CI + ci * nb);
+    }
+  rbo_dbdgemm(fold, Order, TransA, TransB, M, N, K, alpha, A, lda, B, ldb, CI, ldci);
+  for (int i = 0; i < M; i++)
+    for (int j = 0; j < N; j++) {
+      size_t c = row ? (size_t)i * ldc + j : (size_t)j * ldc + i;
+      size_t ci = row ? (size_t)i * ldci + j : (size_t)j * ldci + i;
+      C[c] = rbo_ddbconv(fold, CI + ci * nb);
+    }
+  free(CI);
+}
+
+/* ------------------------------------------------------------------------- */
+/* Exact dot product (not a ReproBLAS routine): TwoProduct via fma splits each   */
+/* product into two doubles exactly; both are added into a 2240-bit two's        */
+/* complement fixed-point accumulator (LSB = 2^-1120), and the total is rounded  */
+/* once, to nearest-even. Valid while no product underflows below 2^-1074+53.    */
+/* ------------------------------------------------------------------------- */
+#define XLIMBS 35
+#define XLSB (-1120)
+
+static void xacc_add(uint64_t *acc, double v) {
+  if (v == 0.0) return;
+  int e;
+  double m = frexp(fabs(v), &e);                 /* |v| = m * 2^e, m in [0.5,1) */
+  uint64_t mant = (uint64_t)ldexp(m, 53);       /* 53-bit integer, |v| = mant*2^(e-53) */
+  int pos = e - 53 - XLSB;                       /* bit position of mant's LSB */
+  int limb = pos / 64, off = pos % 64;
+  uint64_t w[XLIMBS];
+  memset(w, 0, sizeof(w));
+  w[limb] = mant << off;
+  if (off && limb + 1 < XLIMBS) w[limb + 1] = mant >> (64 - off);
+  if (v < 0) { /* two's complement negate */
+    int carry = 1;
+    for (int i = 0; i < XLIMBS; i++) {
+      uint64_t t = ~w[i] + (uint64_t)carry;
+      carry = carry && t == 0;
+      w[i] = t;
+    }
+  }
+  unsigned __int128 c = 0;
+  for (int i = 0; i < XLIMBS; i++) {
+    c += (unsigned __int128)acc[i] + w[i];
+    acc[i] = (uint64_t)c;
+    c >>= 64;
+  }
+}
+
+static double xacc_round(const uint64_t *acc_in) {
+  uint64_t a[XLIMBS];
+  memcpy(a, acc_in, sizeof(a));
+  int neg = (a[XLIMBS - 1] >> 63) & 1;
+  if (neg) {
+    int carry = 1;
+    for (int i = 0; i < XLIMBS; i++) {
+      uint64_t t = ~a[i] + (uint64_t)carry;
+      carry = carry && t == 0;
+      a[i] = t;
+    }
+  }
+  int top = -1;
+  for (int i = XLIMBS - 1; i >= 0 && top < 0; i--)
+    if (a[i]) top = i * 64 + 63 - __builtin_clzll(a[i]);
+  if (top < 0) return 0.0;
+  /* gather 64 bits starting at 'top' downward, plus a sticky bit for the rest */
+  uint64_t hi = 0;
+  int sticky = 0;
+  for (int b = 0; b < 64; b++) {
+    int p = top - b;
+    uint64_t bit = p >= 0 ? (a[p / 64] >> (p % 64)) & 1 : 0;
+    hi = (hi << 1) | bit;
+  }
+  for (int p = top - 64; p >= 0 && !sticky; p--) sticky = (a[p / 64] >> (p % 64)) & 1;
+  uint64_t mant = hi >> 11;                      /* 53 bits */
+  uint64_t rest = hi & 0x7ff;
+  int round_up = rest > 0x400 || (rest == 0x400 && (sticky || (mant & 1)));
+  if (rest == 0x400 && !sticky && !(mant & 1)) round_up = 0;
+  mant += (uint64_t)round_up;
+  double r = ldexp((double)mant, top - 52 + XLSB);
+  return neg ? -r : r;
+}
+
+double rbo_exact_dot(int N, const double *X, int incX, const double *Y, int incY) {
+  uint64_t acc[XLIMBS];
+  memset(acc, 0, sizeof(acc));
+  for (int i = 0; i < N; i++) {
+    double x = X[(size_t)i * incX], y = Y[(size_t)i * incY];
+    double p = x * y;
+    double e = fma(x, y, -p);
+    xacc_add(acc, p);
+    xacc_add(acc, e);
+  }
+  return xacc_round(acc);
+}

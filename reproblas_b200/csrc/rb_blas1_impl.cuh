@@ -1,0 +1,617 @@
+// rb_blas1_impl.cuh -- single-pass persistent binned reductions for sum / dot / sum of squares
+// (FP64, FP32) and complex sum / dotc (FP64 complex, FP32 complex) on sm_100a.
+//
+// One launch does the whole reduction:
+//   1. every thread streams its share of the input (16-byte vector loads over whole
+//      warp tiles; element loads for the ragged head/tail and for strided inputs), and
+//      deposits it into a fold-F binned accumulator held in registers, raising its index
+//      per tile from the tile's largest magnitude (binned_dmdupdate) and renormalising
+//      before the endurance is exceeded (binned_dmrenorm);
+//   2. the accumulators of a warp are merged by a butterfly of binned_dmdmadd over
+//      __shfl_xor_sync, then the warps of the CTA through shared memory;
+//   3. each CTA writes its state to a scratch record and takes an arrival ticket; the
+//      last CTA merges all records (and the caller's accumulator), renormalises, writes
+//      the binned result in the reference layout and its conversion to a scalar, and
+//      resets the ticket.
+// Every merge is exact, so the result does not depend on the grid, the block size, the
+// tile shape, or which CTA arrives last.
+//
+// Reference routines: src/binnedBLAS/dmdsum.ccog:56-90, dmddot.ccog:59-101,
+// dmdssq.ccog:59-101, smssum.ccog, smsdot.ccog:59-100, zmzsum.ccog:56-110,
+// zmzdotc.ccog:58-120, cmcsum.ccog.
+#pragma once
+#include "rb_binned.cuh"
+#include "rb_kernels.cuh"
+
+namespace rb {
+
+// ---------------------------------------------------------------------------------------
+// loads
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ void ldv(const double* p, double (&o)[2]) {
+  double2 v;
+  asm volatile("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];"
+               : "=d"(v.x), "=d"(v.y) : "l"(p));
+  o[0] = v.x; o[1] = v.y;
+}
+__device__ __forceinline__ void ldv(const float* p, float (&o)[4]) {
+  float4 v;
+  asm volatile("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
+  o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+template <typename T> __device__ __forceinline__ T lds(const T* p) { return __ldg(p); }
+
+// Record loads: records written by other CTAs are read from L2 (ld.global.cg); records in
+// shared memory are read with plain loads (a global-space load on a shared address faults).
+template <bool GLOBAL, typename T> __device__ __forceinline__ T ldrec(const T* p) {
+  if constexpr (GLOBAL) return __ldcg(p);
+  else return *p;
+}
+
+// ---------------------------------------------------------------------------------------
+// Sum-of-squares helpers: binned_dscale (src/binned/dscale.c:25-31) and
+// binned_dmdrescale (src/binned/dmdrescale.c:20-37).
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ double dscale_of_key(unsigned key) {
+  int e = (int)(key >> 20);
+  e = e < 40 ? 40 : e;
+  e -= (e - 1022 - 1) % 40;
+  // ldexp(0.5, e - 1022) == 2^(e - 1023): biased exponent e
+  return __longlong_as_double((long long)e << 52);
+}
+
+template <int F>
+__device__ __forceinline__ void rescale(Acc<double, F>& a, double x, double scaleY) {
+  if (x == scaleY || x == 0.0 || scaleY == 0.0) return;
+  if (a.idx == kEmpty) {
+    // dividing an all-zero state reproduces binned_dmdupdate(fold, 0.0) on it
+    a.raise_to(BT<double>::kMaxIndex);
+    return;
+  }
+  double r = __ddiv_rn(x, scaleY);
+  r = __dmul_rn(r, r);
+  bool reset = false;
+#pragma unroll
+  for (int i = 0; i < F; i++) {
+    if (!reset) {
+      a.pri[i] = __ddiv_rn(a.pri[i], r);
+      if (a.pri[i] == 0.0) {
+        reset = true;
+        // binned_dmdupdate(fold - i, 0.0, ...) on the all-zero tail
+#pragma unroll
+        for (int j = 0; j < F; j++)
+          if (j >= i) { a.pri[j] = BT<double>::bin(BT<double>::kMaxIndex + j - i); a.car[j] = 0.0; }
+      }
+    }
+  }
+  a.idx = BT<double>::mindex(a.pri[0]);
+}
+
+// binned_dmdmaddsq (src/binned/dmdmaddsq.c:26-41): Y(scaleY) += X(scaleX)
+template <int F>
+__device__ __forceinline__ void merge_sq(Acc<double, F>& Y, double& sY, Acc<double, F> X, double sX) {
+  if (sX > sY) {
+    rescale(Y, sX, sY);
+    Y.merge(X);
+    sY = sX;
+  } else if (sX == sY) {
+    Y.merge(X);
+  } else {
+    rescale(X, sY, sX);
+    Y.merge(X);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Per-thread state of a real reduction
+// ---------------------------------------------------------------------------------------
+template <typename T, int F, int OP>
+struct Red1 {
+  Acc<T, F> a;
+  double scl;   // sum of squares: current power-of-two scale (0 = none yet)
+
+  __device__ __forceinline__ void init() { a.zero(); scl = 0.0; }
+
+  // Deposit K elements (x[k], y[k]) of which the first nv are real.
+  template <int K>
+  __device__ __forceinline__ void tile(const T (&x)[K], const T (&y)[K], int nv) {
+    if (OP == kOpSum) {
+      a.template tile<K>(x, nv);
+    } else if (OP == kOpDot) {
+      T v[K];
+#pragma unroll
+      for (int k = 0; k < K; k++) v[k] = BT<T>::mul(x[k], y[k]);
+      a.template tile<K>(v, nv);
+    } else {
+      ssq_tile<K>(x, nv);
+    }
+  }
+
+  // dmdssq.ccog:70-101 for one tile
+  template <int K>
+  __device__ __forceinline__ void ssq_tile(const T (&x)[K], int nv) {
+    if (nv <= 0) return;
+    unsigned m = 0;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      unsigned kk = BT<T>::key(x[k]);
+      m = (k < nv && kk > m) ? kk : m;
+    }
+    if (m >= BT<T>::kInfKey) {
+      // the reference adds |x| naively: NaN stays NaN, any infinity becomes +Inf
+#pragma unroll
+      for (int k = 0; k < K; k++)
+        if (k < nv && BT<T>::key(x[k]) >= BT<T>::kInfKey)
+          a.flags |= (x[k] != x[k]) ? kNaN : kPosInf;
+      return;
+    }
+    if constexpr (sizeof(T) == 8) {
+      double nscl = dscale_of_key(m);
+      if (nscl > scl) {
+        if (scl > 0.0) rescale(a, nscl, scl);
+        scl = nscl;
+      }
+      double inv = __ddiv_rn(1.0, scl);
+      double v[K];
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        double t = __dmul_rn(x[k], inv);
+        v[k] = __dmul_rn(t, t);
+      }
+      a.template tile<K>(v, nv);
+    }
+  }
+
+  __device__ __forceinline__ void merge(const Red1& o) {
+    if (OP == kOpSsq) {
+      if constexpr (sizeof(T) == 8) merge_sq(a, scl, o.a, o.scl);
+    } else {
+      a.merge(o.a);
+    }
+  }
+
+  __device__ __forceinline__ Red1 shfl_xor(int mask) const {
+    Red1 o;
+    o.a = a.shfl_xor(mask);
+    o.scl = __shfl_xor_sync(0xffffffffu, scl, mask);
+    return o;
+  }
+
+  // Scratch / shared-memory record: [pri F][car F][flags][scale]
+  __device__ __forceinline__ void save(T* r) const {
+#pragma unroll
+    for (int i = 0; i < F; i++) { r[i] = a.pri[i]; r[F + i] = a.car[i]; }
+    r[2 * F] = BT<T>::from((typename BT<T>::U)a.flags);
+    r[2 * F + 1] = (T)scl;
+  }
+  template <bool G = false>
+  __device__ __forceinline__ void restore(const T* r) {
+#pragma unroll
+    for (int i = 0; i < F; i++) { a.pri[i] = ldrec<G>(r + i); a.car[i] = ldrec<G>(r + F + i); }
+    a.flags = (unsigned)BT<T>::bits(ldrec<G>(r + 2 * F));
+    scl = (double)ldrec<G>(r + 2 * F + 1);
+    a.idx = (a.pri[0] == T(0)) ? kEmpty : BT<T>::mindex(a.pri[0]);
+    a.deposits = 0;
+  }
+};
+
+// ---------------------------------------------------------------------------------------
+// Block-level merge: warp butterflies, then the warps through shared memory. On return
+// thread 0 holds the merge of every thread's state.
+// ---------------------------------------------------------------------------------------
+template <typename S, typename T, int REC>
+__device__ __forceinline__ void block_merge(S& st, T* smem) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+#pragma unroll 1
+  for (int m = 16; m; m >>= 1) st.merge(st.shfl_xor(m));
+  if (lane == 0) st.save(smem + warp * REC);
+  __syncthreads();
+  if (warp == 0) {
+    if (lane < nwarps) st.restore(smem + lane * REC);
+    else st.init();
+#pragma unroll 1
+    for (int m = 16; m; m >>= 1) st.merge(st.shfl_xor(m));
+  }
+  __syncthreads();
+}
+
+// Arrival ticket: returns true in every thread of the last CTA to arrive.
+__device__ __forceinline__ bool arrive_last(unsigned* ticket) {
+  __shared__ unsigned s_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned t = atomicAdd(ticket, 1u);
+    s_last = (t == gridDim.x - 1) ? 1u : 0u;
+  }
+  __syncthreads();
+  bool last = s_last != 0;
+  if (last) __threadfence();
+  return last;
+}
+
+// ---------------------------------------------------------------------------------------
+// Real reduction kernel
+// ---------------------------------------------------------------------------------------
+template <typename T> struct VecW;
+template <> struct VecW<double> { static constexpr int n = 2; };
+template <> struct VecW<float> { static constexpr int n = 4; };
+
+template <typename T, int F, int OP, bool VEC>
+__global__ void __launch_bounds__(256)
+blas1_kernel(Blas1Args args) {
+  constexpr int VW = VecW<T>::n;     // elements per 16-byte vector
+  constexpr int NV = 4;              // vectors per thread per warp tile
+  constexpr int WT = 32 * NV * VW;   // elements per warp tile
+  constexpr int REC = 2 * F + 2;
+  __shared__ T smem[32 * REC];
+
+  const T* __restrict__ x = (const T*)args.x;
+  const T* __restrict__ y = (const T*)args.y;
+  const long long nthreads = (long long)gridDim.x * blockDim.x;
+  const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+
+  Red1<T, F, OP> st;
+  st.init();
+
+  long long head = args.n, body_end = args.n;
+  if (VEC) {
+    head = args.head;
+    body_end = args.body_end;
+    const long long nwt = (body_end - head) / WT;
+    const long long gwarp = gtid >> 5, nwarps = nthreads >> 5;
+#pragma unroll 1
+    for (long long wt = gwarp; wt < nwt; wt += nwarps) {
+      const long long base = head + wt * WT;
+      T xv[NV * VW], yv[NV * VW];
+#pragma unroll
+      for (int k = 0; k < NV; k++) {
+        T t[VW];
+        ldv(x + base + (long long)(k * 32 + lane) * VW, t);
+#pragma unroll
+        for (int j = 0; j < VW; j++) xv[k * VW + j] = t[j];
+      }
+      if (OP == kOpDot) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+          T t[VW];
+          ldv(y + base + (long long)(k * 32 + lane) * VW, t);
+#pragma unroll
+          for (int j = 0; j < VW; j++) yv[k * VW + j] = t[j];
+        }
+      }
+      st.template tile<NV * VW>(xv, yv, NV * VW);
+    }
+  }
+
+  // Element path: the head and tail around the vector body, or everything when the
+  // input is strided or not 16-byte aligned.
+  {
+    const long long S = head + (args.n - body_end);
+    constexpr int K = 4;
+#pragma unroll 1
+    for (long long b = gtid; b < S; b += K * nthreads) {
+      T xv[K], yv[K];
+      int nv = 0;
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        long long i = b + k * nthreads;
+        xv[k] = T(0);
+        yv[k] = T(0);
+        if (i < S) {
+          long long e = i < head ? i : body_end + (i - head);
+          xv[k] = lds(x + e * args.incx);
+          if (OP == kOpDot) yv[k] = lds(y + e * args.incy);
+          nv = k + 1;
+        }
+      }
+      st.template tile<K>(xv, yv, nv);
+    }
+  }
+
+  // Every per-thread state must be renormalised before merging (binned_dmdmadd adds
+  // primaries, which only stays inside the binade for renormalised operands).
+  st.a.renorm();
+  block_merge<Red1<T, F, OP>, T, REC>(st, smem);
+
+  T* records = (T*)args.scratch.records;
+  if (threadIdx.x == 0) st.save(records + (long long)blockIdx.x * REC);
+  if (!arrive_last(args.scratch.ticket)) return;
+
+  // Last CTA: merge every CTA's record.
+  st.init();
+#pragma unroll 1
+  for (int r = threadIdx.x; r < (int)gridDim.x; r += blockDim.x) {
+    Red1<T, F, OP> o;
+    o.template restore<true>(records + (long long)r * REC);
+    st.merge(o);
+  }
+  block_merge<Red1<T, F, OP>, T, REC>(st, smem);
+
+  if (threadIdx.x == 0) {
+    T* acc = (T*)args.acc;
+    if (acc) {
+      Red1<T, F, OP> o;
+      o.a.load(acc, acc + F, 1);
+      o.scl = args.scale ? *args.scale : 0.0;
+      st.merge(o);
+    }
+    st.a.renorm();
+    T outp[F], outc[F];
+    st.a.store(outp, outc, 1);
+    if (acc) {
+#pragma unroll
+      for (int i = 0; i < F; i++) { acc[i] = outp[i]; acc[F + i] = outc[i]; }
+    }
+    double scl = st.scl;
+    if (OP == kOpSsq) {
+      // dmdssq.ccog:4963-4969: a non-finite result reports the scale of 1.0
+      if (st.a.flags) scl = 1.0;
+      if (args.scale) *args.scale = scl;
+    }
+    if (args.result) {
+      if constexpr (sizeof(T) == 8) {
+        double c = conv<F>(outp, outc, 1);
+        if (OP == kOpSsq && args.sqrt_result) c = __dmul_rn(scl, __dsqrt_rn(c));  // rdnrm2.c:31
+        *(double*)args.result = c;
+      } else {
+        *(float*)args.result = sconv<F>(outp, outc, 1);
+      }
+    }
+    *args.scratch.ticket = 0u;
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Complex reduction kernel: two accumulators (real, imaginary) with separate indices
+// (zmzupdate.c:20-23), each component deposited independently.
+// ---------------------------------------------------------------------------------------
+template <typename T, int F, int OP>
+struct RedC {
+  Acc<T, F> re, im;
+  __device__ __forceinline__ void init() { re.zero(); im.zero(); }
+  __device__ __forceinline__ void merge(const RedC& o) { re.merge(o.re); im.merge(o.im); }
+  __device__ __forceinline__ RedC shfl_xor(int m) const {
+    RedC o;
+    o.re = re.shfl_xor(m);
+    o.im = im.shfl_xor(m);
+    return o;
+  }
+  __device__ __forceinline__ void save(T* r) const {
+#pragma unroll
+    for (int i = 0; i < F; i++) {
+      r[i] = re.pri[i]; r[F + i] = re.car[i];
+      r[2 * F + 1 + i] = im.pri[i]; r[3 * F + 1 + i] = im.car[i];
+    }
+    r[2 * F] = BT<T>::from((typename BT<T>::U)re.flags);
+    r[4 * F + 1] = BT<T>::from((typename BT<T>::U)im.flags);
+  }
+  template <bool G = false>
+  __device__ __forceinline__ void restore(const T* r) {
+#pragma unroll
+    for (int i = 0; i < F; i++) {
+      re.pri[i] = ldrec<G>(r + i); re.car[i] = ldrec<G>(r + F + i);
+      im.pri[i] = ldrec<G>(r + 2 * F + 1 + i); im.car[i] = ldrec<G>(r + 3 * F + 1 + i);
+    }
+    re.flags = (unsigned)BT<T>::bits(ldrec<G>(r + 2 * F));
+    im.flags = (unsigned)BT<T>::bits(ldrec<G>(r + 4 * F + 1));
+    re.idx = (re.pri[0] == T(0)) ? kEmpty : BT<T>::mindex(re.pri[0]);
+    im.idx = (im.pri[0] == T(0)) ? kEmpty : BT<T>::mindex(im.pri[0]);
+    re.deposits = im.deposits = 0;
+  }
+};
+
+template <typename T> struct Pair;
+template <> struct Pair<double> {
+  using V = double2;
+  static __device__ __forceinline__ V ld(const double* p) { return __ldg((const double2*)p); }
+};
+template <> struct Pair<float> {
+  using V = float2;
+  static __device__ __forceinline__ V ld(const float* p) { return __ldg((const float2*)p); }
+};
+
+template <typename T, int F, int OP>
+__global__ void __launch_bounds__(256)
+blasc_kernel(Blas1Args args) {
+  constexpr int REC = 4 * F + 2;
+  constexpr int K = 4;   // complex elements per thread per step
+  __shared__ T smem[32 * REC];
+  using B = BT<T>;
+
+  const T* __restrict__ x = (const T*)args.x;
+  const T* __restrict__ y = (const T*)args.y;
+  const long long nthreads = (long long)gridDim.x * blockDim.x;
+  const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+
+  RedC<T, F, OP> st;
+  st.init();
+
+#pragma unroll 1
+  for (long long b = gtid; b < args.n; b += K * nthreads) {
+    if (OP == kOpCSum) {
+      T vr[K], vi[K];
+      int nv = 0;
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        long long i = b + k * nthreads;
+        vr[k] = T(0); vi[k] = T(0);
+        if (i < args.n) {
+          auto v = Pair<T>::ld(x + 2 * i * args.incx);
+          vr[k] = v.x; vi[k] = v.y;
+          nv = k + 1;
+        }
+      }
+      st.re.template tile<K>(vr, nv);
+      st.im.template tile<K>(vi, nv);
+    } else {
+      // conj(x)*y: real part receives xr*yr and xi*yi, imaginary part xr*yi and
+      // -(xi*yr), each product deposited separately (depositDotC.py:14-23)
+      T vr[2 * K], vi[2 * K];
+      int nv = 0;
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        long long i = b + k * nthreads;
+        vr[2 * k] = vr[2 * k + 1] = vi[2 * k] = vi[2 * k + 1] = T(0);
+        if (i < args.n) {
+          auto xv = Pair<T>::ld(x + 2 * i * args.incx);
+          auto yv = Pair<T>::ld(y + 2 * i * args.incy);
+          vr[2 * k] = B::mul(xv.x, yv.x);
+          vr[2 * k + 1] = B::mul(xv.y, yv.y);
+          vi[2 * k] = B::mul(xv.x, yv.y);
+          vi[2 * k + 1] = -B::mul(xv.y, yv.x);
+          nv = 2 * k + 2;
+        }
+      }
+      st.re.template tile<2 * K>(vr, nv);
+      st.im.template tile<2 * K>(vi, nv);
+    }
+  }
+
+  st.re.renorm();
+  st.im.renorm();
+  block_merge<RedC<T, F, OP>, T, REC>(st, smem);
+
+  T* records = (T*)args.scratch.records;
+  if (threadIdx.x == 0) st.save(records + (long long)blockIdx.x * REC);
+  if (!arrive_last(args.scratch.ticket)) return;
+
+  st.init();
+#pragma unroll 1
+  for (int r = threadIdx.x; r < (int)gridDim.x; r += blockDim.x) {
+    RedC<T, F, OP> o;
+    o.template restore<true>(records + (long long)r * REC);
+    st.merge(o);
+  }
+  block_merge<RedC<T, F, OP>, T, REC>(st, smem);
+
+  if (threadIdx.x == 0) {
+    T* acc = (T*)args.acc;   // interleaved: pri re/im (2F), car re/im (2F)
+    if (acc) {
+      RedC<T, F, OP> o;
+      o.re.load(acc, acc + 2 * F, 2);
+      o.im.load(acc + 1, acc + 2 * F + 1, 2);
+      st.merge(o);
+    }
+    st.re.renorm();
+    st.im.renorm();
+    T p[2 * F], c[2 * F];
+    st.re.store(p, c, 2);
+    st.im.store(p + 1, c + 1, 2);
+    if (acc) {
+#pragma unroll
+      for (int i = 0; i < 2 * F; i++) { acc[i] = p[i]; acc[2 * F + i] = c[i]; }
+    }
+    if (args.result) {
+      T* out = (T*)args.result;
+      if constexpr (sizeof(T) == 8) {
+        // zzmconv_sub.c:18-21
+        out[0] = conv<F>(p, c, 2);
+        out[1] = conv<F>(p + 1, c + 1, 2);
+      } else {
+        out[0] = sconv<F>(p, c, 2);
+        out[1] = sconv<F>(p + 1, c + 1, 2);
+      }
+    }
+    *args.scratch.ticket = 0u;
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Merge of `count` double_binned states (device) into `out` (device): the operation
+// binnedMPI's DBDBADD applies per element (src/binnedMPI/DBDBADD.ccog:22-24 ->
+// binned_dbdbaddv -> binned_dmdmadd), done as one CTA tree on the GPU. Used to combine
+// per-GPU partial states after an all-gather.
+// ---------------------------------------------------------------------------------------
+template <int F>
+__global__ void __launch_bounds__(256) merge_states_kernel(int count, const double* states,
+                                                           double* out) {
+  constexpr int REC = 2 * F + 2;
+  __shared__ double smem[32 * REC];
+  Red1<double, F, kOpSum> st;
+  st.init();
+  for (int i = threadIdx.x; i < count; i += blockDim.x) {
+    Red1<double, F, kOpSum> o;
+    o.init();
+    o.a.load(states + (long long)i * 2 * F, states + (long long)i * 2 * F + F, 1);
+    o.a.renorm();
+    st.merge(o);
+  }
+  block_merge<Red1<double, F, kOpSum>, double, REC>(st, smem);
+  if (threadIdx.x == 0) {
+    Red1<double, F, kOpSum> o;
+    o.init();
+    o.a.load(out, out + F, 1);
+    st.merge(o);
+    st.a.renorm();
+    st.a.store(out, out + F, 1);
+  }
+}
+
+
+// Per-fold launchers, instantiated once per fold in rb_blas1_f<F>.cu.
+template <typename T, int F>
+cudaError_t launch_real(int op, bool vec, int grid, int block, const Blas1Args& a,
+                        cudaStream_t s) {
+  if (op == kOpSum) {
+    if (vec) blas1_kernel<T, F, kOpSum, true><<<grid, block, 0, s>>>(a);
+    else blas1_kernel<T, F, kOpSum, false><<<grid, block, 0, s>>>(a);
+  } else if (op == kOpDot) {
+    if (vec) blas1_kernel<T, F, kOpDot, true><<<grid, block, 0, s>>>(a);
+    else blas1_kernel<T, F, kOpDot, false><<<grid, block, 0, s>>>(a);
+  } else if (op == kOpSsq && sizeof(T) == 8) {
+    if (vec) blas1_kernel<T, F, kOpSsq, true><<<grid, block, 0, s>>>(a);
+    else blas1_kernel<T, F, kOpSsq, false><<<grid, block, 0, s>>>(a);
+  } else {
+    return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+template <typename T, int F>
+cudaError_t launch_cplx(int op, int grid, int block, const Blas1Args& a, cudaStream_t s) {
+  if (op == kOpCSum) blasc_kernel<T, F, kOpCSum><<<grid, block, 0, s>>>(a);
+  else if (op == kOpCDotc && sizeof(T) == 8) blasc_kernel<T, F, kOpCDotc><<<grid, block, 0, s>>>(a);
+  else return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+template <int F>
+cudaError_t launch_merge(int count, const double* states, double* out, cudaStream_t s) {
+  merge_states_kernel<F><<<1, 256, 0, s>>>(count, states, out);
+  return cudaGetLastError();
+}
+
+template <typename T, int F>
+const void* real_kernel_ptr(int op, bool vec) {
+  if (op == kOpSum) return vec ? (const void*)blas1_kernel<T, F, kOpSum, true> : (const void*)blas1_kernel<T, F, kOpSum, false>;
+  if (op == kOpDot) return vec ? (const void*)blas1_kernel<T, F, kOpDot, true> : (const void*)blas1_kernel<T, F, kOpDot, false>;
+  if (sizeof(T) == 8) return vec ? (const void*)blas1_kernel<T, F, kOpSsq, true> : (const void*)blas1_kernel<T, F, kOpSsq, false>;
+  return nullptr;
+}
+
+template <int F>
+const void* blas1_kernel_ptr(char type, int op, bool vec) {
+  switch (type) {
+    case 'd': return real_kernel_ptr<double, F>(op, vec);
+    case 's': return real_kernel_ptr<float, F>(op, vec);
+    case 'z': return op == kOpCSum ? (const void*)blasc_kernel<double, F, kOpCSum> : (const void*)blasc_kernel<double, F, kOpCDotc>;
+    default: return (const void*)blasc_kernel<float, F, kOpCSum>;
+  }
+}
+
+template <int F>
+Blas1FoldOps make_fold_ops() {
+  Blas1FoldOps o;
+  o.real_d = launch_real<double, F>;
+  o.real_s = launch_real<float, F>;
+  o.cplx_z = launch_cplx<double, F>;
+  o.cplx_c = launch_cplx<float, F>;
+  o.merge = launch_merge<F>;
+  o.kernel = blas1_kernel_ptr<F>;
+  return o;
+}
+
+}  // namespace rb

@@ -1,0 +1,81 @@
+// rb_host.h -- host-side runtime shared by the C ABI translation units: the thread-local
+// error channel and stream, per-(device, stream) workspaces, pointer classification and
+// launch-shape selection.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <cstdio>
+#include <mutex>
+#include <string>
+
+#include "rb_kernels.cuh"
+
+namespace rb {
+
+// ---- error channel ------------------------------------------------------------------
+void set_error(int code, const std::string& msg);
+bool cuda_ok(cudaError_t e, const char* what);   // records RB_ERR_CUDA and returns false
+
+// ---- current stream / launch shape / counters -----------------------------------------
+cudaStream_t current_stream();
+void count_launch(unsigned n = 1);
+struct LaunchShape { int ctas_per_sm; int threads; };
+LaunchShape launch_shape();   // user override or defaults (0 = default)
+
+struct DeviceInfo { int device; int sms; };
+bool device_info(DeviceInfo* out);
+
+// ---- pointers ---------------------------------------------------------------------------
+enum class Mem { Device, Pinned, Pageable };
+Mem classify(const void* p);
+inline bool on_device(const void* p) { return classify(p) == Mem::Device; }
+
+// ---- workspace ----------------------------------------------------------------------------
+// One per (device, stream). Holds the grid-reduction scratch, a device accumulator and
+// result slots for value-returning calls, pinned host slots for small transfers, and a
+// lazily allocated ring of staging buffers for host inputs. Calls lock `mu` for their whole
+// duration, so concurrent calls on one stream from several host threads are serialised.
+struct Workspace {
+  std::mutex mu;
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;   // H2D staging copies (non-blocking)
+  GridScratch scratch{};                // records + ticket
+  size_t records_bytes = 0;
+  unsigned char* dsmall = nullptr;      // device: accumulator / scale / result slots
+  unsigned char* hsmall = nullptr;      // pinned host mirror of dsmall
+  static constexpr size_t kSmallBytes = 4096;
+  // staging ring: kRing slots, each with up to two operand buffers of chunk_bytes
+  static constexpr int kRing = 3;
+  size_t chunk_bytes = 0;
+  unsigned char* ring[kRing][2] = {};
+  cudaEvent_t copied[kRing] = {};
+  cudaEvent_t consumed[kRing] = {};
+  bool ring_ready = false;
+  // grow-on-demand device buffer for larger per-call temporaries (gemv/gemm partials)
+  unsigned char* big = nullptr;
+  size_t big_bytes = 0;
+
+  double* dacc() { return (double*)dsmall; }                  // 1024 B accumulator slot
+  double* dscale() { return (double*)(dsmall + 1024); }        // 8 B
+  void* dresult() { return (void*)(dsmall + 1088); }           // 64 B result slot
+  double* hacc() { return (double*)hsmall; }
+  double* hscale() { return (double*)(hsmall + 1024); }
+  void* hresult() { return (void*)(hsmall + 1088); }
+
+  bool ensure_ring(size_t chunk);
+  bool ensure_big(size_t bytes);
+};
+
+// Locked workspace of the calling thread's current device and stream, or nullptr (error set).
+Workspace* acquire_workspace(std::unique_lock<std::mutex>* lock);
+
+// Grid size for a reduction over `work` elements with `elems_per_thread` per thread.
+int reduction_grid(long long work, int elems_per_thread, int threads, int occupancy_per_sm);
+
+// Occupancy of the reduction kernels (CTAs per SM) for the chosen launch shape.
+int blas1_occupancy(char type, int fold, int op, bool vec, int threads);
+
+}  // namespace rb

@@ -1,0 +1,81 @@
+// rb_kernels.cuh -- launch-parameter structs and kernel entry points shared between the
+// CUDA translation units and the host-side C ABI (rb_api.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace rb {
+
+// Real-valued BLAS1 reductions (one binned accumulator per result)
+enum Op1 : int {
+  kOpSum = 0,   // sum x_i                       (dmdsum / smssum)
+  kOpDot = 1,   // sum fl(x_i * y_i)             (dmddot / smsdot)
+  kOpSsq = 2,   // sum fl((x_i * (1/scl))^2)     (dmdssq), running power-of-two scale
+};
+// Complex BLAS1 reductions (two accumulators, real and imaginary)
+enum OpC : int {
+  kOpCSum = 0,   // sum x_i                      (zmzsum / cmcsum)
+  kOpCDotc = 1,  // sum conj(x_i) * y_i          (zmzdotc)
+};
+
+// Workspace used by a grid-wide reduction: one partial record per CTA plus an arrival
+// ticket. The last CTA to arrive merges the records and resets the ticket to zero.
+struct GridScratch {
+  void* records;       // >= gridDim.x * record_bytes
+  unsigned* ticket;    // zero on entry, zero again on exit
+};
+
+struct Blas1Args {
+  long long n;               // number of elements
+  const void* x;             // device pointer
+  long long incx;            // stride in elements (>= 0)
+  const void* y;             // device pointer (dot only)
+  long long incy;
+  long long head;            // vector path: elements before the aligned body
+  long long body_end;        // vector path: end of the body of whole warp tiles
+  GridScratch scratch;
+  void* acc;                 // device binned accumulator (reference layout), read then written
+  double* scale;             // ssq: device scale, read then written (may be null: 0)
+  void* result;              // device converted result (T, or 2 T for complex); may be null
+  int sqrt_result;           // ssq: write scale*sqrt(conv) instead of conv
+};
+
+// Launch helpers implemented in rb_blas1.cu; return cudaSuccess or the launch error.
+// `vec` selects the 16-byte vector body (contiguous, aligned inputs).
+cudaError_t launch_blas1_d(int fold, int op, bool vec, int grid, int block,
+                           const Blas1Args& a, cudaStream_t s);
+cudaError_t launch_blas1_s(int fold, int op, bool vec, int grid, int block,
+                           const Blas1Args& a, cudaStream_t s);
+cudaError_t launch_blas1_z(int fold, int op, int grid, int block, const Blas1Args& a,
+                           cudaStream_t s);
+cudaError_t launch_blas1_c(int fold, int op, int grid, int block, const Blas1Args& a,
+                           cudaStream_t s);
+
+// out (device double_binned) += each of `count` device double_binned states.
+cudaError_t launch_merge_states(int fold, int count, const double* states, double* out,
+                                cudaStream_t s);
+
+// Bytes of one per-CTA record for the given element size, fold and component count.
+inline size_t blas1_record_bytes(size_t elem, int fold, int comps) {
+  // per component: fold primaries, fold carries, flags word, scale (ssq)
+  size_t per = (2 * (size_t)fold + 2) * elem;
+  if (per < 16) per = 16;
+  return ((comps * per) + 15) / 16 * 16 + 16;
+}
+
+// Launchers of one fold (instantiated in rb_blas1_f<F>.cu)
+struct Blas1FoldOps {
+  cudaError_t (*real_d)(int op, bool vec, int grid, int block, const Blas1Args& a, cudaStream_t s);
+  cudaError_t (*real_s)(int op, bool vec, int grid, int block, const Blas1Args& a, cudaStream_t s);
+  cudaError_t (*cplx_z)(int op, int grid, int block, const Blas1Args& a, cudaStream_t s);
+  cudaError_t (*cplx_c)(int op, int grid, int block, const Blas1Args& a, cudaStream_t s);
+  cudaError_t (*merge)(int count, const double* states, double* out, cudaStream_t s);
+  const void* (*kernel)(char type, int op, bool vec);
+};
+extern const Blas1FoldOps blas1_fold2, blas1_fold3, blas1_fold4, blas1_fold5, blas1_fold6,
+    blas1_fold7, blas1_fold8;
+
+bool fold_supported(int fold);
+constexpr int kMaxFold = 8;
+
+}  // namespace rb

@@ -1,0 +1,186 @@
+// rb_runtime.cu -- host runtime: error channel, streams, workspaces, pointer classification.
+#include <map>
+#include <memory>
+#include <utility>
+
+#include "rb_host.h"
+#include "../../include/reproblas_b200.h"
+
+namespace rb {
+
+// ---- error channel ----------------------------------------------------------------------
+static thread_local int t_err = RB_SUCCESS;
+static thread_local std::string t_msg;
+
+void set_error(int code, const std::string& msg) {
+  t_err = code;
+  t_msg = msg;
+  if (std::getenv("RB_VERBOSE")) std::fprintf(stderr, "reproblas_b200: %s\n", msg.c_str());
+}
+
+bool cuda_ok(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return true;
+  set_error(RB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  return false;
+}
+
+// ---- stream / launch shape / counters ----------------------------------------------------
+static thread_local cudaStream_t t_stream = nullptr;
+static std::atomic<int> g_ctas_per_sm{0};
+static std::atomic<int> g_threads{0};
+static std::atomic<unsigned long long> g_launches{0};
+
+cudaStream_t current_stream() { return t_stream; }
+void count_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+LaunchShape launch_shape() { return LaunchShape{g_ctas_per_sm.load(), g_threads.load()}; }
+
+bool device_info(DeviceInfo* out) {
+  static std::mutex mu;
+  static std::map<int, int> sms;
+  int dev = 0;
+  if (!cuda_ok(cudaGetDevice(&dev), "cudaGetDevice")) return false;
+  std::lock_guard<std::mutex> g(mu);
+  auto it = sms.find(dev);
+  if (it == sms.end()) {
+    int n = 0;
+    if (!cuda_ok(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev),
+                 "cudaDeviceGetAttribute"))
+      return false;
+    it = sms.emplace(dev, n).first;
+  }
+  out->device = dev;
+  out->sms = it->second;
+  return true;
+}
+
+// ---- pointers -------------------------------------------------------------------------------
+Mem classify(const void* p) {
+  if (!p) return Mem::Pageable;
+  cudaPointerAttributes a;
+  cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();   // unregistered host memory on old runtimes
+    return Mem::Pageable;
+  }
+  switch (a.type) {
+    case cudaMemoryTypeDevice:
+    case cudaMemoryTypeManaged: return Mem::Device;
+    case cudaMemoryTypeHost: return Mem::Pinned;
+    default: return Mem::Pageable;
+  }
+}
+
+// ---- workspace ------------------------------------------------------------------------------
+bool Workspace::ensure_ring(size_t chunk) {
+  if (ring_ready && chunk <= chunk_bytes) return true;
+  for (int i = 0; i < kRing; i++)
+    for (int j = 0; j < 2; j++)
+      if (ring[i][j]) { cudaFree(ring[i][j]); ring[i][j] = nullptr; }
+  for (int i = 0; i < kRing; i++) {
+    for (int j = 0; j < 2; j++)
+      if (cudaMalloc(&ring[i][j], chunk) != cudaSuccess) {
+        set_error(RB_ERR_ALLOC, "staging buffer allocation failed");
+        return false;
+      }
+    if (!copied[i] && !cuda_ok(cudaEventCreateWithFlags(&copied[i], cudaEventDisableTiming), "event")) return false;
+    if (!consumed[i] && !cuda_ok(cudaEventCreateWithFlags(&consumed[i], cudaEventDisableTiming), "event")) return false;
+  }
+  chunk_bytes = chunk;
+  ring_ready = true;
+  return true;
+}
+
+bool Workspace::ensure_big(size_t bytes) {
+  if (bytes <= big_bytes) return true;
+  if (big) { cudaFree(big); big = nullptr; big_bytes = 0; }
+  if (cudaMalloc(&big, bytes) != cudaSuccess) {
+    set_error(RB_ERR_ALLOC, "workspace allocation failed");
+    return false;
+  }
+  big_bytes = bytes;
+  return true;
+}
+
+static bool init_workspace(Workspace* w, int dev, cudaStream_t s, int sms) {
+  w->device = dev;
+  w->stream = s;
+  // records for up to 16 CTAs per SM of the largest record (complex, fold 8)
+  size_t rec = blas1_record_bytes(8, kMaxFold, 2);
+  w->records_bytes = (size_t)sms * 16 * rec;
+  if (cudaMalloc(&w->scratch.records, w->records_bytes) != cudaSuccess ||
+      cudaMalloc(&w->scratch.ticket, 256) != cudaSuccess ||
+      cudaMalloc(&w->dsmall, Workspace::kSmallBytes) != cudaSuccess) {
+    set_error(RB_ERR_ALLOC, "workspace allocation failed");
+    return false;
+  }
+  if (!cuda_ok(cudaMemset(w->scratch.ticket, 0, 256), "cudaMemset")) return false;
+  if (!cuda_ok(cudaMallocHost(&w->hsmall, Workspace::kSmallBytes), "cudaMallocHost")) return false;
+  if (!cuda_ok(cudaStreamCreateWithFlags(&w->copy_stream, cudaStreamNonBlocking),
+               "cudaStreamCreate"))
+    return false;
+  return true;
+}
+
+Workspace* acquire_workspace(std::unique_lock<std::mutex>* lock) {
+  static std::mutex mu;
+  static std::map<std::pair<int, cudaStream_t>, std::unique_ptr<Workspace>> table;
+  DeviceInfo di;
+  if (!device_info(&di)) return nullptr;
+  cudaStream_t s = current_stream();
+  Workspace* w = nullptr;
+  {
+    std::lock_guard<std::mutex> g(mu);
+    auto key = std::make_pair(di.device, s);
+    auto it = table.find(key);
+    if (it == table.end()) {
+      std::unique_ptr<Workspace> nw(new Workspace());
+      if (!init_workspace(nw.get(), di.device, s, di.sms)) return nullptr;
+      it = table.emplace(key, std::move(nw)).first;
+    }
+    w = it->second.get();
+  }
+  *lock = std::unique_lock<std::mutex>(w->mu);
+  return w;
+}
+
+int reduction_grid(long long work, int elems_per_thread, int threads, int occupancy_per_sm) {
+  DeviceInfo di;
+  if (!device_info(&di)) return 1;
+  LaunchShape ls = launch_shape();
+  int per_sm = ls.ctas_per_sm > 0 ? ls.ctas_per_sm : occupancy_per_sm;
+  if (per_sm < 1) per_sm = 1;
+  if (per_sm > 16) per_sm = 16;
+  long long max_grid = (long long)di.sms * per_sm;
+  long long need = (work + (long long)threads * elems_per_thread - 1) /
+                   ((long long)threads * elems_per_thread);
+  if (need < 1) need = 1;
+  return (int)(need < max_grid ? need : max_grid);
+}
+
+}  // namespace rb
+
+// ---- C ABI: controls -------------------------------------------------------------------------
+extern "C" {
+
+int rb_get_last_error(void) { return rb::t_err; }
+const char* rb_get_last_error_message(void) { return rb::t_msg.c_str(); }
+void rb_clear_error(void) {
+  rb::t_err = RB_SUCCESS;
+  rb::t_msg.clear();
+}
+void rb_set_stream(void* stream) { rb::t_stream = (cudaStream_t)stream; }
+void* rb_get_stream(void) { return (void*)rb::t_stream; }
+void rb_set_launch_config(int ctas_per_sm, int threads_per_cta) {
+  if (threads_per_cta < 0 || threads_per_cta > 256 || (threads_per_cta % 32) != 0 ||
+      ctas_per_sm < 0 || ctas_per_sm > 16) {
+    rb::set_error(RB_ERR_INVALID_ARG, "rb_set_launch_config: threads must be a multiple of 32 "
+                                      "in [32, 256] (or 0), CTAs per SM in [1, 16] (or 0)");
+    return;
+  }
+  rb::g_ctas_per_sm.store(ctas_per_sm);
+  rb::g_threads.store(threads_per_cta);
+}
+unsigned long long rb_kernel_launch_count(void) { return rb::g_launches.load(); }
+const char* rb_version(void) { return "reproblas_b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

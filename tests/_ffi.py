@@ -1,0 +1,115 @@
+"""ctypes bindings used by the tests: the oracle restatement (port), the reference library
+compiled from its own sources (ref, optional), and the product's C ABI.
+
+The oracle libraries are test infrastructure; the product library is what is checked.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PORT_SO = os.path.join(ROOT, "oracle", "_build", "librb_oracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libreproblas_ref.so")
+
+c_int, c_double, c_float, c_char, c_vp = (ctypes.c_int, ctypes.c_double, ctypes.c_float,
+                                          ctypes.c_char, ctypes.c_void_p)
+
+
+def ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+_SIGS = {
+    # name: (restype, argtypes) -- shared by the port (rbo_ prefix) and the reference
+    "dbdsum": (None, [c_int, c_int, c_vp, c_int, c_vp]),
+    "dbddot": (None, [c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp]),
+    "dbdssq": (c_double, [c_int, c_int, c_vp, c_int, c_double, c_vp]),
+    "sbssum": (None, [c_int, c_int, c_vp, c_int, c_vp]),
+    "sbsdot": (None, [c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp]),
+    "zbzsum": (None, [c_int, c_int, c_vp, c_int, c_vp]),
+    "zbzdotc": (None, [c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp]),
+    "cbcsum": (None, [c_int, c_int, c_vp, c_int, c_vp]),
+    "dbdgemv": (None, [c_int, c_char, c_char, c_int, c_int, c_double, c_vp, c_int, c_vp, c_int,
+                       c_vp, c_int]),
+    "dbdgemm": (None, [c_int, c_char, c_char, c_char, c_int, c_int, c_int, c_double, c_vp, c_int,
+                       c_vp, c_int, c_vp, c_int]),
+    "rdsum": (c_double, [c_int, c_int, c_vp, c_int]),
+    "rddot": (c_double, [c_int, c_int, c_vp, c_int, c_vp, c_int]),
+    "rdnrm2": (c_double, [c_int, c_int, c_vp, c_int]),
+    "rssum": (c_float, [c_int, c_int, c_vp, c_int]),
+    "rsdot": (c_float, [c_int, c_int, c_vp, c_int, c_vp, c_int]),
+    "rzsum_sub": (None, [c_int, c_int, c_vp, c_int, c_vp]),
+    "rzdotc_sub": (None, [c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp]),
+    "rcsum_sub": (None, [c_int, c_int, c_vp, c_int, c_vp]),
+    "rdgemv": (None, [c_int, c_char, c_char, c_int, c_int, c_double, c_vp, c_int, c_vp, c_int,
+                      c_double, c_vp, c_int]),
+    "rdgemm": (None, [c_int, c_char, c_char, c_char, c_int, c_int, c_int, c_double, c_vp, c_int,
+                      c_vp, c_int, c_double, c_vp, c_int]),
+    "dbdbadd": (None, [c_int, c_vp, c_vp]),
+    "dbdconv": (None, [c_int, c_double, c_vp]),
+    "ddbconv": (c_double, [c_int, c_vp]),
+    "dbdbaddsq": (c_double, [c_int, c_double, c_vp, c_double, c_vp]),
+    "dbbound": (c_double, [c_int, c_int, c_double, c_double]),
+    "dscale": (c_double, [c_double]),
+    "dindex": (c_int, [c_double]),
+    "sindex": (c_int, [c_float]),
+    "sbsbadd": (None, [c_int, c_vp, c_vp]),
+    "ssbconv": (c_float, [c_int, c_vp]),
+}
+
+# reference-library names for the shared signatures
+_REF_NAMES = {
+    "dbdsum": "binnedBLAS_dbdsum", "dbddot": "binnedBLAS_dbddot", "dbdssq": "binnedBLAS_dbdssq",
+    "sbssum": "binnedBLAS_sbssum", "sbsdot": "binnedBLAS_sbsdot", "zbzsum": "binnedBLAS_zbzsum",
+    "zbzdotc": "binnedBLAS_zbzdotc", "cbcsum": "binnedBLAS_cbcsum",
+    "dbdgemv": "binnedBLAS_dbdgemv", "dbdgemm": "binnedBLAS_dbdgemm",
+    "rdsum": "reproBLAS_rdsum", "rddot": "reproBLAS_rddot", "rdnrm2": "reproBLAS_rdnrm2",
+    "rssum": "reproBLAS_rssum", "rsdot": "reproBLAS_rsdot", "rzsum_sub": "reproBLAS_rzsum_sub",
+    "rzdotc_sub": "reproBLAS_rzdotc_sub", "rcsum_sub": "reproBLAS_rcsum_sub",
+    "rdgemv": "reproBLAS_rdgemv", "rdgemm": "reproBLAS_rdgemm",
+    "dbdbadd": "binned_dbdbadd", "dbdconv": "binned_dbdconv", "ddbconv": "binned_ddbconv",
+    "dbdbaddsq": "binned_dbdbaddsq", "dbbound": "binned_dbbound", "dscale": "binned_dscale",
+    "dindex": "binned_dindex", "sindex": "binned_sindex", "sbsbadd": "binned_sbsbadd",
+    "ssbconv": "binned_ssbconv",
+}
+
+
+class _Lib:
+    def __init__(self, path, names):
+        self.path = path
+        self.lib = ctypes.CDLL(path)
+        for key, (res, args) in _SIGS.items():
+            fn = getattr(self.lib, names(key))
+            fn.restype = res
+            fn.argtypes = args
+            setattr(self, key, fn)
+
+
+_port = None
+_ref = None
+
+
+def port():
+    global _port
+    if _port is None:
+        _port = _Lib(PORT_SO, lambda k: "rbo_" + k)
+        extra = _port.lib.rbo_exact_dot
+        extra.restype = c_double
+        extra.argtypes = [c_int, c_vp, c_int, c_vp, c_int]
+        _port.exact_dot = extra
+    return _port
+
+
+def ref():
+    """The reference library compiled from its own sources, or None when absent."""
+    global _ref
+    if _ref is None and os.path.exists(REF_SO):
+        _ref = _Lib(REF_SO, lambda k: _REF_NAMES[k])
+    return _ref
+
+
+def binned_zeros(fold, kind="d", n=1):
+    per = {"d": 2 * fold, "z": 4 * fold, "s": 2 * fold, "c": 4 * fold}[kind]
+    dt = np.float64 if kind in "dz" else np.float32
+    return np.zeros(per * n, dtype=dt)

@@ -1,0 +1,133 @@
+"""Generate the golden fixtures in this directory from the ReproBLAS reference library
+itself, compiled from its own sources by `make -C oracle ref` (oracle/_ref/).
+
+Inputs are regenerated from (distribution, n, seed) by tests/_data.py; the fixture stores
+a SHA-256 of each input so that a change in the generator is detected rather than
+silently compared. Outputs are the reference's binned states and converted results.
+
+Usage: python tests/golden/make_golden.py   (needs oracle/_ref/libreproblas_ref.so)
+"""
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+from _ffi import ref, ptr, binned_zeros  # noqa: E402
+from _data import gen, gen_complex, blas23_operands  # noqa: E402
+
+DISTS = ["uniform", "normal", "loguniform", "illcond", "sine", "bigsmall", "huge", "tiny"]
+NS = [1, 7, 1000, 4095, 20000]
+FOLDS = [2, 3, 4]
+
+
+def h(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()[:16]
+
+
+def hexb(a):
+    return np.ascontiguousarray(a).tobytes().hex()
+
+
+def main():
+    R = ref()
+    if R is None:
+        sys.exit("oracle/_ref/libreproblas_ref.so not built (make -C oracle ref)")
+    cases = []
+    for dist in DISTS:
+        for n in NS:
+            x = gen(dist, n, 11)
+            y = gen(dist, n, 12)
+            xf = gen(dist, n, 11, np.float32)
+            yf = gen(dist, n, 12, np.float32)
+            xz = gen_complex(dist, n, 11)
+            yz = gen_complex(dist, n, 12)
+            xc = gen_complex(dist, n, 11, np.complex64)
+            hashes = {"x": h(x), "y": h(y), "xf": h(xf), "yf": h(yf), "xz": h(xz),
+                      "yz": h(yz), "xc": h(xc)}
+            for fold in FOLDS:
+                c = {"dist": dist, "n": n, "fold": fold, "hash": hashes}
+                z = binned_zeros(fold); R.dbdsum(fold, n, ptr(x), 1, ptr(z)); c["dbdsum"] = hexb(z)
+                c["rdsum"] = hexb(np.float64(R.rdsum(fold, n, ptr(x), 1)))
+                z = binned_zeros(fold); R.dbddot(fold, n, ptr(x), 1, ptr(y), 1, ptr(z)); c["dbddot"] = hexb(z)
+                c["rddot"] = hexb(np.float64(R.rddot(fold, n, ptr(x), 1, ptr(y), 1)))
+                z = binned_zeros(fold); s = R.dbdssq(fold, n, ptr(x), 1, 0.0, ptr(z))
+                c["dbdssq"] = hexb(z); c["dbdssq_scale"] = hexb(np.float64(s))
+                c["rdnrm2"] = hexb(np.float64(R.rdnrm2(fold, n, ptr(x), 1)))
+                z = binned_zeros(fold, "s"); R.sbssum(fold, n, ptr(xf), 1, ptr(z)); c["sbssum"] = hexb(z)
+                c["rssum"] = hexb(np.float32(R.rssum(fold, n, ptr(xf), 1)))
+                z = binned_zeros(fold, "s"); R.sbsdot(fold, n, ptr(xf), 1, ptr(yf), 1, ptr(z)); c["sbsdot"] = hexb(z)
+                c["rsdot"] = hexb(np.float32(R.rsdot(fold, n, ptr(xf), 1, ptr(yf), 1)))
+                z = binned_zeros(fold, "z"); R.zbzsum(fold, n, ptr(xz), 1, ptr(z)); c["zbzsum"] = hexb(z)
+                o = np.zeros(2); R.rzsum_sub(fold, n, ptr(xz), 1, ptr(o)); c["rzsum"] = hexb(o)
+                z = binned_zeros(fold, "z"); R.zbzdotc(fold, n, ptr(xz), 1, ptr(yz), 1, ptr(z)); c["zbzdotc"] = hexb(z)
+                o = np.zeros(2); R.rzdotc_sub(fold, n, ptr(xz), 1, ptr(yz), 1, ptr(o)); c["rzdotc"] = hexb(o)
+                z = binned_zeros(fold, "c"); R.cbcsum(fold, n, ptr(xc), 1, ptr(z)); c["cbcsum"] = hexb(z)
+                o = np.zeros(2, np.float32); R.rcsum_sub(fold, n, ptr(xc), 1, ptr(o)); c["rcsum"] = hexb(o)
+                cases.append(c)
+
+    # The dsum configuration quoted by the benchmark: N = 2^20, fold 3, sine and uniform
+    cfg0 = []
+    for dist in ["sine", "uniform"]:
+        x = gen(dist, 1 << 20, 0)
+        z = binned_zeros(3); R.dbdsum(3, 1 << 20, ptr(x), 1, ptr(z))
+        cfg0.append({"dist": dist, "n": 1 << 20, "seed": 0, "hash": h(x), "dbdsum": hexb(z),
+                     "rdsum": hexb(np.float64(R.rdsum(3, 1 << 20, ptr(x), 1)))})
+
+    # Inf / NaN vectors (the reference's validate_internal_daugsum Inf/NaN fills, N=255)
+    special = []
+    rng = np.random.default_rng(3)
+    for k in range(12):
+        x = rng.uniform(-1, 1, 255)
+        pos = rng.choice(255, size=1 + k % 3, replace=False)
+        vals = [np.inf, -np.inf, np.nan][k % 3:] + [np.inf, -np.inf, np.nan][:k % 3]
+        for p, v in zip(pos, vals):
+            x[p] = v
+        y = np.ones(255)
+        special.append({"x": hexb(x),
+                        "rdsum": hexb(np.float64(R.rdsum(3, 255, ptr(x), 1))),
+                        "rddot": hexb(np.float64(R.rddot(3, 255, ptr(x), 1, ptr(y), 1))),
+                        "rdnrm2": hexb(np.float64(R.rdnrm2(3, 255, ptr(x), 1)))})
+
+    # Small gemv / gemm (all orders and transposes), alpha 1.5, beta 0.5, fold 3.
+    # Operands are regenerated from blas23_operands(seed) and checked by hash.
+    blas23 = []
+    seed = 1000
+    for order in "rc":
+        for ta in "nt":
+            M, N = 37, 53
+            A, xv, yv = blas23_operands(seed, M * N, 64, 64)
+            lda = N if order == "r" else M
+            yo = yv.copy()
+            R.rdgemv(3, order.encode(), ta.encode(), M, N, 1.5, ptr(A), lda, ptr(xv), 1, 0.5, ptr(yo), 1)
+            blas23.append({"kind": "gemv", "order": order, "ta": ta, "M": M, "N": N, "lda": lda,
+                           "seed": seed, "hash": h(np.concatenate([A, xv, yv])), "out": hexb(yo)})
+            seed += 1
+            for tb in "nt":
+                M, N, K = 19, 23, 41
+                A, B, C = blas23_operands(seed, M * K, K * N, M * N)
+                if order == "r":
+                    lda = K if ta == "n" else M; ldb = N if tb == "n" else K; ldc = N
+                else:
+                    lda = M if ta == "n" else K; ldb = K if tb == "n" else N; ldc = M
+                Co = C.copy()
+                R.rdgemm(3, order.encode(), ta.encode(), tb.encode(), M, N, K, 1.5, ptr(A), lda,
+                         ptr(B), ldb, 0.5, ptr(Co), ldc)
+                blas23.append({"kind": "gemm", "order": order, "ta": ta, "tb": tb, "M": M, "N": N,
+                               "K": K, "lda": lda, "ldb": ldb, "ldc": ldc, "seed": seed,
+                               "hash": h(np.concatenate([A, B, C])), "out": hexb(Co)})
+                seed += 1
+
+    out = {"generator": "tests/golden/make_golden.py", "reference": "ReproBLAS v2.1.0 "
+           "compiled by oracle/Makefile (gcc -std=c99 -O3 -march=x86-64-v3)",
+           "blas1": cases, "dsum_config": cfg0, "special": special, "blas23": blas23}
+    with open(os.path.join(HERE, "reference_golden.json"), "w") as f:
+        json.dump(out, f, separators=(",", ":"))
+    print("wrote", len(cases), "blas1 cases,", len(special), "special,", len(blas23), "blas2/3")
+
+
+if __name__ == "__main__":
+    main()
