@@ -165,6 +165,27 @@ unsigned long long rb_kernel_launch_count(void);
 int rb_dbdbadd_states(const int fold, const int count, const double_binned *states,
                       double_binned *out);
 
+/* Reproducible dot product that allocates nothing. No counterpart in the reference.
+ * For callers that may not allocate device memory where they need the dot product:
+ * plugins whose host application owns the whole device-memory budget, and
+ * latency-critical code (an MPI reduction callback, a real-time loop) that cannot afford
+ * cudaMalloc/cudaFree, which may synchronise the device. The other entry points allocate
+ * a per-stream workspace on first use.
+ * Same arithmetic and bits as binnedBLAS_dbddot / reproBLAS_rddot. X and Y must be device
+ * memory; Z (a device double_binned, accumulated into as by binnedBLAS_dbddot) and result
+ * (a device double receiving the converted sum) may each be NULL. Work is enqueued on
+ * `stream` (a cudaStream_t; NULL = legacy default stream) and not waited for.
+ * Scratch: a fixed 128 KiB device array inside this library, one per GPU that loads it,
+ * held until exit; it holds (128 KiB - 256 B) / ((2*fold + 2) * 8 B) CTA records, and a
+ * launch shape needing more (see rb_set_launch_config) is rejected with
+ * RB_ERR_INVALID_ARG. The first call on each device looks the array's address up
+ * (cudaGetSymbolAddress); make it before any stream capture. All calls share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller.
+ * Returns an RB_* code. */
+int rb_ddot_noalloc(const int fold, const int N, const double *X, const int incX,
+                    const double *Y, const int incY, double_binned *Z, double *result,
+                    void *stream);
+
 /* Library version string. */
 const char *rb_version(void);
 
