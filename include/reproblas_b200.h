@@ -95,6 +95,30 @@ void reproBLAS_rcsum_sub(const int fold, const int N, const void *X, const int i
                          void *sum);
 void reproBLAS_csum_sub(const int N, const void *X, const int incX, void *sum);
 
+/* include/reproBLAS.h:49 (src/reproBLAS/rdgemv.c:35-87):
+ * y <- conv(binned(beta*y) + sum_j A_ij * fl(alpha*x_j)); Order 'r'/'R' row-major, else
+ * column-major; TransA 'n'/'N' no transpose, else transpose. */
+void reproBLAS_rdgemv(const int fold, const char Order, const char TransA, const int M,
+                      const int N, const double alpha, const double *A, const int lda,
+                      const double *X, const int incX, const double beta, double *Y,
+                      const int incY);
+/* include/reproBLAS.h:119 (src/reproBLAS/dgemv.c:32), fold 3 */
+void reproBLAS_dgemv(const char Order, const char TransA, const int M, const int N,
+                     const double alpha, const double *A, const int lda, const double *X,
+                     const int incX, const double beta, double *Y, const int incY);
+
+/* include/reproBLAS.h:54 (src/reproBLAS/rdgemm.c:41-105):
+ * C <- conv(binned(beta*C) + sum_k fl(fl(alpha*A_ik) * B_kj)), products rounded in FP64. */
+void reproBLAS_rdgemm(const int fold, const char Order, const char TransA, const char TransB,
+                      const int M, const int N, const int K, const double alpha,
+                      const double *A, const int lda, const double *B, const int ldb,
+                      const double beta, double *C, const int ldc);
+/* include/reproBLAS.h:124 (src/reproBLAS/dgemm.c:38), fold 3 */
+void reproBLAS_dgemm(const char Order, const char TransA, const char TransB, const int M,
+                     const int N, const int K, const double alpha, const double *A,
+                     const int lda, const double *B, const int ldb, const double beta,
+                     double *C, const int ldc);
+
 /* ------------------------------------------------------------------------------------
  * binnedBLAS level: add into a caller-owned binned accumulator (resumable state).
  * include/binnedBLAS.h
@@ -125,6 +149,18 @@ void binnedBLAS_zbzdotc(const int fold, const int N, const void *X, const int in
 /* include/binnedBLAS.h:76 (src/binnedBLAS/cbcsum.c -> cmcsum.ccog) */
 void binnedBLAS_cbcsum(const int fold, const int N, const void *X, const int incX,
                        float_complex_binned *Y);
+
+/* include/binnedBLAS.h:87 (src/binnedBLAS/dbdgemv.ccog:57-162): Y (binned states, stride
+ * incY states) += A*fl(alpha*x) or A^T*fl(alpha*x) */
+void binnedBLAS_dbdgemv(const int fold, const char Order, const char TransA, const int M,
+                        const int N, const double alpha, const double *A, const int lda,
+                        const double *X, const int incX, double_binned *Y, const int incY);
+/* include/binnedBLAS.h:92 (src/binnedBLAS/dbdgemm.ccog:61-420): C (binned states, leading
+ * dimension ldc in states) += op(fl(alpha*A)) * op(B) */
+void binnedBLAS_dbdgemm(const int fold, const char Order, const char TransA, const char TransB,
+                        const int M, const int N, const int K, const double alpha,
+                        const double *A, const int lda, const double *B, const int ldb,
+                        double_binned *C, const int ldc);
 
 /* ------------------------------------------------------------------------------------
  * B200 controls (no reference counterpart)

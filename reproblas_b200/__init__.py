@@ -51,6 +51,19 @@ SIGNATURES = {
     "binnedBLAS_zbzsum": (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp]),
     "binnedBLAS_zbzdotc": (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp, _c_int, _c_vp]),
     "binnedBLAS_cbcsum": (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp]),
+    "reproBLAS_rdgemv": (None, [_c_int, _c_char, _c_char, _c_int, _c_int, _c_double, _c_vp,
+                                _c_int, _c_vp, _c_int, _c_double, _c_vp, _c_int]),
+    "reproBLAS_dgemv": (None, [_c_char, _c_char, _c_int, _c_int, _c_double, _c_vp, _c_int,
+                               _c_vp, _c_int, _c_double, _c_vp, _c_int]),
+    "reproBLAS_rdgemm": (None, [_c_int, _c_char, _c_char, _c_char, _c_int, _c_int, _c_int,
+                                _c_double, _c_vp, _c_int, _c_vp, _c_int, _c_double, _c_vp,
+                                _c_int]),
+    "reproBLAS_dgemm": (None, [_c_char, _c_char, _c_char, _c_int, _c_int, _c_int, _c_double,
+                               _c_vp, _c_int, _c_vp, _c_int, _c_double, _c_vp, _c_int]),
+    "binnedBLAS_dbdgemv": (None, [_c_int, _c_char, _c_char, _c_int, _c_int, _c_double, _c_vp,
+                                  _c_int, _c_vp, _c_int, _c_vp, _c_int]),
+    "binnedBLAS_dbdgemm": (None, [_c_int, _c_char, _c_char, _c_char, _c_int, _c_int, _c_int,
+                                  _c_double, _c_vp, _c_int, _c_vp, _c_int, _c_vp, _c_int]),
     "rb_get_last_error": (_c_int, []),
     "rb_get_last_error_message": (ctypes.c_char_p, []),
     "rb_clear_error": (None, []),

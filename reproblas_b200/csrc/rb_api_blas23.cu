@@ -1,0 +1,287 @@
+// rb_api_blas23.cu -- C ABI for the binned dgemv / dgemm (reproBLAS_* / binnedBLAS_* names).
+//
+// Both orders and transposes are mapped onto the kernels' canonical forms the way the
+// reference does it: column-major is row-major with the transpose flipped
+// (src/binnedBLAS/dbdgemv.ccog:146-158); dgemm uses general operand strides. Host operands
+// are copied to a device workspace first; outputs are copied back before returning.
+#include <cstring>
+
+#include "rb_host.h"
+#include "../../include/reproblas_b200.h"
+
+namespace rb {
+namespace {
+
+const Blas23FoldOps* ops23(int fold) {
+  switch (fold) {
+    case 2: return &blas23_fold2;
+    case 3: return &blas23_fold3;
+    case 4: return &blas23_fold4;
+    case 5: return &blas23_fold5;
+    case 6: return &blas23_fold6;
+    case 7: return &blas23_fold7;
+    case 8: return &blas23_fold8;
+    default: return nullptr;
+  }
+}
+
+bool is_row(char o) { return o == 'r' || o == 'R'; }
+bool is_nt(char t) { return t == 'n' || t == 'N'; }
+
+// Bump allocator over the workspace's big buffer (one call at a time holds the workspace).
+struct Bump {
+  unsigned char* base;
+  size_t off = 0;
+  void* take(size_t bytes) {
+    void* p = base + off;
+    off += (bytes + 255) / 256 * 256;
+    return p;
+  }
+};
+
+// Bytes spanned by `count` elements of `elem` bytes with stride `inc` elements.
+size_t span(long long count, long long inc, size_t elem) {
+  if (count <= 0) return 0;
+  return ((size_t)(count - 1) * (size_t)inc + 1) * elem;
+}
+
+// Make `p` (spanning `bytes`) available on the device: device pointers are used in place,
+// host ones are copied into the bump region.
+const void* to_device(const void* p, size_t bytes, Bump* b, cudaStream_t s, bool* ok) {
+  if (!p || bytes == 0 || on_device(p)) return p;
+  void* d = b->take(bytes);
+  if (!cuda_ok(cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, s), "copy operand")) *ok = false;
+  return d;
+}
+
+struct GemvReq {
+  int fold;
+  char order, trans;
+  int M, N;
+  double alpha;
+  const double* A;
+  int lda;
+  const double* X;
+  int incX;
+  double beta;
+  double* Y;        // values (kOutValue) or binned states (kOutBinned)
+  int incY;
+  int mode;
+};
+
+bool run_gemv(const GemvReq& q) {
+  if (q.M == 0 || q.N == 0) return true;   // rdgemv.c:43-45
+  const Blas23FoldOps* o = ops23(q.fold);
+  if (!o) { set_error(RB_ERR_INVALID_ARG, "fold must be in [2, 8]"); return false; }
+  if (q.M < 0 || q.N < 0 || q.lda < 1 || q.incX < 0 || q.incY < 1) {
+    set_error(RB_ERR_INVALID_ARG, "gemv: negative size, lda < 1, incX < 0 or incY < 1");
+    return false;
+  }
+  // row-major view of the stored matrix: Rs rows x Cs columns
+  bool nt = is_nt(q.trans);
+  long long Rs = q.M, Cs = q.N;
+  if (!is_row(q.order)) { Rs = q.N; Cs = q.M; nt = !nt; }
+  if (q.lda < Cs) { set_error(RB_ERR_INVALID_ARG, "gemv: lda smaller than the row length"); return false; }
+  const long long nout = nt ? Rs : Cs, nred = nt ? Cs : Rs;
+  const long long nred_eff = q.alpha == 0.0 ? 0 : nred;   // dbdgemv.ccog:70-72
+  if (q.mode == kOutBinned && nred_eff == 0) return true;  // binnedBLAS_dbdgemv touches nothing
+
+  std::unique_lock<std::mutex> lock;
+  Workspace* w = acquire_workspace(&lock);
+  if (!w) return false;
+  cudaStream_t s = w->stream;
+
+  const size_t per_out = q.mode == kOutValue ? 8 : (size_t)2 * q.fold * 8;
+  const size_t a_bytes = nred_eff > 0 ? ((size_t)(Rs - 1) * q.lda + Cs) * 8 : 0;
+  const size_t x_bytes = span(nred_eff, q.incX, 8);
+  const size_t y_bytes = q.mode == kOutValue ? span(nout, q.incY, 8)
+                                             : ((size_t)(nout - 1) * q.incY + 1) * per_out;
+  // column kernel partials
+  int col_blocks = 0, nchunks = 1;
+  size_t part_bytes = 0;
+  DeviceInfo di;
+  if (!device_info(&di)) return false;
+  if (!nt) {
+    col_blocks = (int)((nout + 255) / 256);
+    long long target = (long long)di.sms * 4;
+    long long ch = (target + col_blocks - 1) / col_blocks;
+    long long maxch = (nred_eff + 15) / 16;
+    if (ch > maxch) ch = maxch;
+    if (ch < 1) ch = 1;
+    nchunks = (int)ch;
+    part_bytes = (size_t)nchunks * nout * (2 * q.fold + 1) * 8;
+    if (!w->ensure_tickets((size_t)col_blocks)) return false;
+  }
+  const bool a_host = a_bytes && !on_device(q.A), x_host = x_bytes && !on_device(q.X);
+  const bool y_host = !on_device(q.Y);
+  size_t need = part_bytes + (a_host ? a_bytes : 0) + (x_host ? x_bytes : 0) +
+                (y_host ? y_bytes : 0) + 4 * 256;
+  if (!w->ensure_big(need)) return false;
+  Bump b{w->big};
+  bool ok = true;
+  const double* dA = (const double*)to_device(q.A, a_bytes, &b, s, &ok);
+  const double* dX = (const double*)to_device(q.X, x_bytes, &b, s, &ok);
+  double* dY = (double*)to_device(q.Y, y_bytes, &b, s, &ok);
+  double* part = part_bytes ? (double*)b.take(part_bytes) : nullptr;
+  if (!ok) return false;
+
+  GemvArgs g{};
+  g.A = dA;
+  g.lda = q.lda;
+  g.x = dX;
+  g.incx = q.incX;
+  g.alpha = q.alpha;
+  g.beta = q.beta;
+  g.mode = q.mode;
+  g.y = q.mode == kOutValue ? dY : nullptr;
+  g.ybin = q.mode == kOutBinned ? dY : nullptr;
+  g.incy = q.incY;
+  count_launch();
+  cudaError_t e;
+  if (nt) {
+    g.R = nout;
+    g.C = nred_eff;
+    long long target_warps = (long long)di.sms * 32;
+    int S = 1;
+    while (S < 8 && nout * S < target_warps) S *= 2;
+    g.split = S;
+    const int rows_per_cta = 8 / S;
+    dim3 grid((unsigned)((nout + rows_per_cta - 1) / rows_per_cta));
+    e = o->gemv(g, true, grid, s);
+  } else {
+    g.C = nout;
+    g.R = nred_eff;
+    g.split = 1;
+    g.scratch = part;
+    g.tickets = w->tickets;
+    dim3 grid((unsigned)col_blocks, (unsigned)nchunks);
+    e = o->gemv(g, false, grid, s);
+  }
+  if (!cuda_ok(e, "gemv launch")) return false;
+  if (y_host) {
+    if (!cuda_ok(cudaMemcpyAsync(q.Y, dY, y_bytes, cudaMemcpyDeviceToHost, s), "copy y") ||
+        !cuda_ok(cudaStreamSynchronize(s), "cudaStreamSynchronize"))
+      return false;
+  }
+  return true;
+}
+
+struct GemmReq {
+  int fold;
+  char order, ta, tb;
+  int M, N, K;
+  double alpha;
+  const double* A;
+  int lda;
+  const double* B;
+  int ldb;
+  double beta;
+  double* C;       // values or binned states
+  int ldc;
+  int mode;
+};
+
+bool run_gemm(const GemmReq& q) {
+  if (q.M == 0 || q.N == 0) return true;   // rdgemm.c:50-52
+  const Blas23FoldOps* o = ops23(q.fold);
+  if (!o) { set_error(RB_ERR_INVALID_ARG, "fold must be in [2, 8]"); return false; }
+  if (q.M < 0 || q.N < 0 || q.K < 0 || q.lda < 1 || q.ldb < 1 || q.ldc < 1) {
+    set_error(RB_ERR_INVALID_ARG, "gemm: negative size or leading dimension < 1");
+    return false;
+  }
+  const bool row = is_row(q.order), ta = !is_nt(q.ta), tb = !is_nt(q.tb);
+  GemmArgs g{};
+  g.M = q.M;
+  g.N = q.N;
+  g.K = (q.alpha == 0.0) ? 0 : q.K;   // dbdgemm.ccog:78-80
+  if (row) {
+    g.sai = ta ? 1 : q.lda;  g.sak = ta ? q.lda : 1;
+    g.sbk = tb ? 1 : q.ldb;  g.sbj = tb ? q.ldb : 1;
+    g.sci = q.ldc;           g.scj = 1;
+  } else {
+    g.sai = ta ? q.lda : 1;  g.sak = ta ? 1 : q.lda;
+    g.sbk = tb ? q.ldb : 1;  g.sbj = tb ? 1 : q.ldb;
+    g.sci = 1;               g.scj = q.ldc;
+  }
+  g.alpha = q.alpha;
+  g.beta = q.beta;
+  g.mode = q.mode;
+  if (q.mode == kOutBinned && g.K == 0) return true;   // binnedBLAS_dbdgemm touches nothing
+
+  std::unique_lock<std::mutex> lock;
+  Workspace* w = acquire_workspace(&lock);
+  if (!w) return false;
+  cudaStream_t s = w->stream;
+  const size_t per = q.mode == kOutValue ? 8 : (size_t)2 * q.fold * 8;
+  const size_t a_bytes = g.K ? ((size_t)(g.M - 1) * g.sai + (size_t)(g.K - 1) * g.sak + 1) * 8 : 0;
+  const size_t b_bytes = g.K ? ((size_t)(g.K - 1) * g.sbk + (size_t)(g.N - 1) * g.sbj + 1) * 8 : 0;
+  const size_t c_bytes = ((size_t)(g.M - 1) * g.sci + (size_t)(g.N - 1) * g.scj + 1) * per;
+  const bool a_host = a_bytes && !on_device(q.A), b_host = b_bytes && !on_device(q.B);
+  const bool c_host = !on_device(q.C);
+  size_t need = (a_host ? a_bytes : 0) + (b_host ? b_bytes : 0) + (c_host ? c_bytes : 0) + 3 * 256;
+  if (need > 3 * 256 && !w->ensure_big(need)) return false;
+  Bump bm{w->big};
+  bool ok = true;
+  g.A = (const double*)to_device(q.A, a_bytes, &bm, s, &ok);
+  g.B = (const double*)to_device(q.B, b_bytes, &bm, s, &ok);
+  double* dC = (double*)to_device(q.C, c_bytes, &bm, s, &ok);
+  if (!ok) return false;
+  g.C = q.mode == kOutValue ? dC : nullptr;
+  g.Cbin = q.mode == kOutBinned ? dC : nullptr;
+  count_launch();
+  if (!cuda_ok(o->gemm(g, s, nullptr, nullptr), "gemm launch")) return false;
+  if (c_host) {
+    if (!cuda_ok(cudaMemcpyAsync(q.C, dC, c_bytes, cudaMemcpyDeviceToHost, s), "copy C") ||
+        !cuda_ok(cudaStreamSynchronize(s), "cudaStreamSynchronize"))
+      return false;
+  }
+  return true;
+}
+
+}  // namespace
+}  // namespace rb
+
+extern "C" {
+
+void reproBLAS_rdgemv(const int fold, const char Order, const char TransA, const int M,
+                      const int N, const double alpha, const double* A, const int lda,
+                      const double* X, const int incX, const double beta, double* Y,
+                      const int incY) {
+  rb::GemvReq q{fold, Order, TransA, M, N, alpha, A, lda, X, incX, beta, Y, incY, rb::kOutValue};
+  rb::run_gemv(q);
+}
+void reproBLAS_dgemv(const char Order, const char TransA, const int M, const int N,
+                     const double alpha, const double* A, const int lda, const double* X,
+                     const int incX, const double beta, double* Y, const int incY) {
+  reproBLAS_rdgemv(3, Order, TransA, M, N, alpha, A, lda, X, incX, beta, Y, incY);
+}
+void binnedBLAS_dbdgemv(const int fold, const char Order, const char TransA, const int M,
+                        const int N, const double alpha, const double* A, const int lda,
+                        const double* X, const int incX, double_binned* Y, const int incY) {
+  rb::GemvReq q{fold, Order, TransA, M, N, alpha, A, lda, X, incX, 1.0, Y, incY, rb::kOutBinned};
+  rb::run_gemv(q);
+}
+void reproBLAS_rdgemm(const int fold, const char Order, const char TransA, const char TransB,
+                      const int M, const int N, const int K, const double alpha, const double* A,
+                      const int lda, const double* B, const int ldb, const double beta,
+                      double* C, const int ldc) {
+  rb::GemmReq q{fold, Order, TransA, TransB, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc,
+                rb::kOutValue};
+  rb::run_gemm(q);
+}
+void reproBLAS_dgemm(const char Order, const char TransA, const char TransB, const int M,
+                     const int N, const int K, const double alpha, const double* A,
+                     const int lda, const double* B, const int ldb, const double beta,
+                     double* C, const int ldc) {
+  reproBLAS_rdgemm(3, Order, TransA, TransB, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+void binnedBLAS_dbdgemm(const int fold, const char Order, const char TransA, const char TransB,
+                        const int M, const int N, const int K, const double alpha,
+                        const double* A, const int lda, const double* B, const int ldb,
+                        double_binned* C, const int ldc) {
+  rb::GemmReq q{fold, Order, TransA, TransB, M, N, K, alpha, A, lda, B, ldb, 1.0, C, ldc,
+                rb::kOutBinned};
+  rb::run_gemm(q);
+}
+
+}  // extern "C"

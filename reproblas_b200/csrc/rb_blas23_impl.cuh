@@ -1,0 +1,333 @@
+// rb_blas23_impl.cuh -- binned dgemv and plain binned dgemm on sm_100a.
+//
+// Every output entry is one binned dot product, so the state of each entry depends only on
+// the multiset of its products (plus the beta*y / beta*C initial value), exactly as in the
+// reference, where the entry is accumulated by blocked binnedBLAS_dbddot calls:
+//   dgemv  y_i <- conv( binned(beta*y_i) + sum_j fl(A_ij * fl(alpha*x_j)) )
+//          (src/reproBLAS/rdgemv.c:35-87, src/binnedBLAS/dbdgemv.ccog:57-162: alpha scales x)
+//   dgemm  C_ij <- conv( binned(beta*C_ij) + sum_k fl(fl(alpha*A_ik) * B_kj) )
+//          (src/reproBLAS/rdgemm.c:41-105, src/binnedBLAS/dbdgemm.ccog:61-420: alpha scales A)
+// beta == 0 starts from the empty state, beta == 1 from binned(y) without a multiply, other
+// betas from binned(fl(y*beta)); alpha == 1 skips the alpha multiply; alpha == 0 deposits no
+// products (the host passes an empty reduction).
+#pragma once
+#include "rb_binned.cuh"
+#include "rb_kernels.cuh"
+
+namespace rb {
+
+// Initial state of an output entry (rdgemv.c:47-57 / rdgemm.c:57-75): binned_dbdconv of
+// beta*y, or of y when beta == 1, or the empty state when beta == 0.
+template <int F>
+__device__ __forceinline__ void init_from_value(Acc<double, F>& a, double y, double beta) {
+  a.zero();
+  if (beta == 0.0) return;
+  double v[1] = {beta == 1.0 ? y : __dmul_rn(y, beta)};
+  a.template tile<1>(v, 1);
+  a.renorm();
+}
+
+// Epilogue shared by the BLAS2/3 kernels: combine the products' state `a` (renormalised)
+// with the entry's initial state and write the result.
+template <int F>
+__device__ __forceinline__ void finish_entry(Acc<double, F>& a, int mode, double* out_value,
+                                             double beta, double* out_binned) {
+  if (mode == kOutValue) {
+    Acc<double, F> init;
+    init_from_value(init, *out_value, beta);
+    init.merge(a);
+    init.renorm();
+    double p[F], c[F];
+    init.store(p, c, 1);
+    *out_value = conv<F>(p, c, 1);
+  } else {
+    Acc<double, F> prev;
+    prev.load(out_binned, out_binned + F, 1);
+    prev.merge(a);
+    prev.renorm();
+    prev.store(out_binned, out_binned + F, 1);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// gemv, reduction along contiguous rows: out_r = sum_c A[r*lda + c] * bx_c, r < R, c < C.
+// S warps share a row (S = 1, 2, 4, 8); a CTA of 8 warps covers 8/S rows.
+// ---------------------------------------------------------------------------------------
+template <int F>
+__global__ void __launch_bounds__(256) gemv_rows_kernel(GemvArgs g) {
+  __shared__ double smem[8 * (2 * F + 2)];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int S = g.split;
+  const int rows_per_cta = 8 / S;
+  const int rloc = warp / S, part = warp % S;
+  const long long r = (long long)blockIdx.x * rows_per_cta + rloc;
+  Acc<double, F> a;
+  a.zero();
+  if (r < g.R) {
+    const double* row = g.A + r * g.lda;
+    const long long chunk = (g.C + S - 1) / S;
+    const long long c0 = part * chunk;
+    const long long c1 = c0 + chunk < g.C ? c0 + chunk : g.C;
+    constexpr int K = 4;
+#pragma unroll 1
+    for (long long b = c0 + lane; b < c1; b += 32 * K) {
+      double v[K];
+      int nv = 0;
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        long long c = b + 32 * k;
+        v[k] = 0.0;
+        if (c < c1) {
+          double xv = __ldg(g.x + c * g.incx);
+          if (g.alpha != 1.0) xv = __dmul_rn(xv, g.alpha);
+          v[k] = __dmul_rn(__ldg(row + c), xv);
+          nv = k + 1;
+        }
+      }
+      a.template tile<K>(v, nv);
+    }
+  }
+  a.renorm();
+#pragma unroll 1
+  for (int m = 16; m; m >>= 1) a.merge(a.shfl_xor(m));
+  constexpr int REC = 2 * F + 2;
+  if (lane == 0) {
+    double* rec = smem + warp * REC;
+#pragma unroll
+    for (int i = 0; i < F; i++) { rec[i] = a.pri[i]; rec[F + i] = a.car[i]; }
+    rec[2 * F] = __longlong_as_double((long long)a.flags);
+  }
+  __syncthreads();
+  if (threadIdx.x < rows_per_cta) {
+    const long long rr = (long long)blockIdx.x * rows_per_cta + threadIdx.x;
+    if (rr < g.R) {
+      Acc<double, F> t;
+      t.zero();
+      for (int p = 0; p < S; p++) {
+        const double* rec = smem + (threadIdx.x * S + p) * REC;
+        Acc<double, F> o;
+        o.zero();
+#pragma unroll
+        for (int i = 0; i < F; i++) { o.pri[i] = rec[i]; o.car[i] = rec[F + i]; }
+        o.flags = (unsigned)__double_as_longlong(rec[2 * F]);
+        o.idx = o.pri[0] == 0.0 ? kEmpty : BT<double>::mindex(o.pri[0]);
+        t.merge(o);
+      }
+      finish_entry<F>(t, g.mode, g.y + rr * g.incy, g.beta,
+                      g.ybin + rr * g.incy * 2 * F);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// gemv, reduction along strided columns: out_c = sum_r A[r*lda + c] * bx_r, c < C, r < R.
+// grid = (column blocks of 256, row chunks). Each thread owns one column of one chunk;
+// partial states go to scratch (structure of arrays), and the last chunk-CTA to arrive for
+// a column block merges them.
+// ---------------------------------------------------------------------------------------
+template <int F>
+__global__ void __launch_bounds__(256) gemv_cols_kernel(GemvArgs g) {
+  constexpr int NF = 2 * F + 1;   // pri, car, flags
+  const long long c = (long long)blockIdx.x * 256 + threadIdx.x;
+  const int chunk = blockIdx.y, nchunks = gridDim.y;
+  const long long rows_per = (g.R + nchunks - 1) / nchunks;
+  const long long r0 = (long long)chunk * rows_per;
+  const long long r1 = r0 + rows_per < g.R ? r0 + rows_per : g.R;
+  Acc<double, F> a;
+  a.zero();
+  if (c < g.C) {
+    constexpr int K = 4;
+#pragma unroll 1
+    for (long long b = r0; b < r1; b += K) {
+      double v[K];
+      int nv = 0;
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        long long r = b + k;
+        v[k] = 0.0;
+        if (r < r1) {
+          double xv = __ldg(g.x + r * g.incx);
+          if (g.alpha != 1.0) xv = __dmul_rn(xv, g.alpha);
+          v[k] = __dmul_rn(__ldg(g.A + r * g.lda + c), xv);
+          nv = k + 1;
+        }
+      }
+      a.template tile<K>(v, nv);
+    }
+    a.renorm();
+    // scratch layout: field f, chunk, column  -> coalesced across the warp
+    double* s = g.scratch;
+    const long long stride = (long long)nchunks * g.C;
+#pragma unroll
+    for (int i = 0; i < F; i++) {
+      s[(long long)i * stride + (long long)chunk * g.C + c] = a.pri[i];
+      s[(long long)(F + i) * stride + (long long)chunk * g.C + c] = a.car[i];
+    }
+    s[(long long)(2 * F) * stride + (long long)chunk * g.C + c] = __longlong_as_double((long long)a.flags);
+  }
+  // last chunk-CTA of this column block merges
+  __shared__ unsigned s_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned t = atomicAdd(g.tickets + blockIdx.x, 1u);
+    s_last = (t == (unsigned)nchunks - 1) ? 1u : 0u;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (c < g.C) {
+    const double* s = g.scratch;
+    const long long stride = (long long)nchunks * g.C;
+    Acc<double, F> t;
+    t.zero();
+    for (int ch = 0; ch < nchunks; ch++) {
+      Acc<double, F> o;
+      o.zero();
+#pragma unroll
+      for (int i = 0; i < F; i++) {
+        o.pri[i] = __ldcg(s + (long long)i * stride + (long long)ch * g.C + c);
+        o.car[i] = __ldcg(s + (long long)(F + i) * stride + (long long)ch * g.C + c);
+      }
+      o.flags = (unsigned)__double_as_longlong(__ldcg(s + (long long)(2 * F) * stride + (long long)ch * g.C + c));
+      o.idx = o.pri[0] == 0.0 ? kEmpty : BT<double>::mindex(o.pri[0]);
+      t.merge(o);
+    }
+    finish_entry<F>(t, g.mode, g.y + c * g.incy, g.beta, g.ybin + c * g.incy * 2 * F);
+  }
+  if (threadIdx.x == 0) g.tickets[blockIdx.x] = 0u;
+  (void)NF;
+}
+
+// ---------------------------------------------------------------------------------------
+// Plain binned dgemm. CTA tile BM x BN of C entries, TM x TN entries per thread, each with
+// its own fold-F accumulator in registers; K in tiles of BK through shared memory, with
+// fl(alpha*A) formed when the A tile is stored. Operands use general strides
+//   op(A)_ik = A[i*sai + k*sak], op(B)_kj = B[k*sbk + j*sbj], C_ij = C[i*sci + j*scj]
+// which cover both orders and both transposes.
+// ---------------------------------------------------------------------------------------
+template <int F, int TM, int TN>
+struct GemmCfg {
+  static constexpr int TX = 16, TY = 16;            // 256 threads
+  static constexpr int BM = TY * TM, BN = TX * TN;
+  static constexpr int BK = 32;
+};
+
+template <int F, int TM, int TN>
+__global__ void __launch_bounds__(256) gemm_kernel(GemmArgs g) {
+  using Cfg = GemmCfg<F, TM, TN>;
+  constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK;
+  __shared__ double As[BK][BM + 1];
+  __shared__ double Bs[BK][BN + 1];
+  const int tid = threadIdx.x;
+  const int tx = tid % Cfg::TX, ty = tid / Cfg::TX;
+  const long long m0 = (long long)blockIdx.y * BM, n0 = (long long)blockIdx.x * BN;
+
+  Acc<double, F> acc[TM][TN];
+#pragma unroll
+  for (int i = 0; i < TM; i++)
+#pragma unroll
+    for (int j = 0; j < TN; j++) acc[i][j].zero();
+
+  const bool a_k_fast = g.sak == 1;   // which stride is unit decides the load order
+  const bool b_j_fast = g.sbj == 1;
+
+#pragma unroll 1
+  for (long long k0 = 0; k0 < g.K; k0 += BK) {
+    // A tile: BM x BK
+#pragma unroll 1
+    for (int e = tid; e < BM * BK; e += 256) {
+      int i, k;
+      if (a_k_fast) { k = e % BK; i = e / BK; } else { i = e % BM; k = e / BM; }
+      const long long gi = m0 + i, gk = k0 + k;
+      double v = 0.0;
+      if (gi < g.M && gk < g.K) {
+        v = __ldg(g.A + gi * g.sai + gk * g.sak);
+        if (g.alpha != 1.0) v = __dmul_rn(v, g.alpha);
+      }
+      As[k][i] = v;
+    }
+    // B tile: BK x BN
+#pragma unroll 1
+    for (int e = tid; e < BK * BN; e += 256) {
+      int k, j;
+      if (b_j_fast) { j = e % BN; k = e / BN; } else { k = e % BK; j = e / BK; }
+      const long long gk = k0 + k, gj = n0 + j;
+      double v = 0.0;
+      if (gk < g.K && gj < g.N) v = __ldg(g.B + gk * g.sbk + gj * g.sbj);
+      Bs[k][j] = v;
+    }
+    __syncthreads();
+    const int kmax = (g.K - k0) < BK ? (int)(g.K - k0) : BK;
+#pragma unroll 1
+    for (int kk = 0; kk < BK; kk += 4) {
+      if (kk >= kmax) break;
+      const int nv = (kmax - kk) < 4 ? (kmax - kk) : 4;
+      double av[TM][4], bv[TN][4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+#pragma unroll
+        for (int i = 0; i < TM; i++) av[i][q] = As[kk + q][ty + i * Cfg::TY];
+#pragma unroll
+        for (int j = 0; j < TN; j++) bv[j][q] = Bs[kk + q][tx + j * Cfg::TX];
+      }
+#pragma unroll
+      for (int i = 0; i < TM; i++)
+#pragma unroll
+        for (int j = 0; j < TN; j++) {
+          double p[4];
+#pragma unroll
+          for (int q = 0; q < 4; q++) p[q] = __dmul_rn(av[i][q], bv[j][q]);
+          acc[i][j].template tile<4>(p, nv);
+        }
+    }
+    __syncthreads();
+  }
+
+#pragma unroll
+  for (int i = 0; i < TM; i++)
+#pragma unroll
+    for (int j = 0; j < TN; j++) {
+      const long long gi = m0 + ty + i * Cfg::TY, gj = n0 + tx + j * Cfg::TX;
+      if (gi < g.M && gj < g.N) {
+        acc[i][j].renorm();
+        const long long off = gi * g.sci + gj * g.scj;
+        finish_entry<F>(acc[i][j], g.mode, g.C + off, g.beta, g.Cbin + off * 2 * F);
+      }
+    }
+}
+
+template <int F>
+cudaError_t launch_gemv(const GemvArgs& g, bool rows, dim3 grid, cudaStream_t s) {
+  if (rows) gemv_rows_kernel<F><<<grid, 256, 0, s>>>(g);
+  else gemv_cols_kernel<F><<<grid, 256, 0, s>>>(g);
+  return cudaGetLastError();
+}
+
+template <int F>
+cudaError_t launch_gemm(const GemmArgs& g, cudaStream_t s, int* bm, int* bn) {
+  if constexpr (F <= 4) {
+    using Cfg = GemmCfg<F, 2, 2>;
+    dim3 grid((unsigned)((g.N + Cfg::BN - 1) / Cfg::BN), (unsigned)((g.M + Cfg::BM - 1) / Cfg::BM));
+    if (bm) *bm = Cfg::BM;
+    if (bn) *bn = Cfg::BN;
+    gemm_kernel<F, 2, 2><<<grid, 256, 0, s>>>(g);
+  } else {
+    using Cfg = GemmCfg<F, 1, 1>;
+    dim3 grid((unsigned)((g.N + Cfg::BN - 1) / Cfg::BN), (unsigned)((g.M + Cfg::BM - 1) / Cfg::BM));
+    if (bm) *bm = Cfg::BM;
+    if (bn) *bn = Cfg::BN;
+    gemm_kernel<F, 1, 1><<<grid, 256, 0, s>>>(g);
+  }
+  return cudaGetLastError();
+}
+
+template <int F>
+Blas23FoldOps make_blas23_ops() {
+  Blas23FoldOps o;
+  o.gemv = launch_gemv<F>;
+  o.gemm = launch_gemm<F>;
+  return o;
+}
+
+}  // namespace rb

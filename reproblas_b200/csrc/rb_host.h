@@ -54,9 +54,13 @@ struct Workspace {
   cudaEvent_t copied[kRing] = {};
   cudaEvent_t consumed[kRing] = {};
   bool ring_ready = false;
-  // grow-on-demand device buffer for larger per-call temporaries (gemv/gemm partials)
+  // grow-on-demand device buffer for larger per-call temporaries (gemv/gemm partials,
+  // device copies of host operands)
   unsigned char* big = nullptr;
   size_t big_bytes = 0;
+  // arrival tickets for multi-CTA merges (zero between calls; kernels reset them)
+  unsigned* tickets = nullptr;
+  size_t ntickets = 0;
 
   double* dacc() { return (double*)dsmall; }                  // 1024 B accumulator slot
   double* dscale() { return (double*)(dsmall + 1024); }        // 8 B
@@ -67,6 +71,7 @@ struct Workspace {
 
   bool ensure_ring(size_t chunk);
   bool ensure_big(size_t bytes);
+  bool ensure_tickets(size_t n);
 };
 
 // Locked workspace of the calling thread's current device and stream, or nullptr (error set).

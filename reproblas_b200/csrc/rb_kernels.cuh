@@ -75,6 +75,48 @@ struct Blas1FoldOps {
 extern const Blas1FoldOps blas1_fold2, blas1_fold3, blas1_fold4, blas1_fold5, blas1_fold6,
     blas1_fold7, blas1_fold8;
 
+// ---- BLAS2/3 ------------------------------------------------------------------------
+enum OutMode : int {
+  kOutValue = 0,    // reproBLAS_r*: init from beta*y (values), write converted values
+  kOutBinned = 1,   // binnedBLAS_dbd*: merge into the caller's binned states
+};
+
+struct GemvArgs {
+  long long R, C;             // rows kernel: R outputs x C reduction; cols kernel: C outputs x R
+  const double* A;
+  long long lda;
+  const double* x;
+  long long incx;
+  double alpha, beta;
+  int mode;
+  double* y;                  // kOutValue: values (stride incy)
+  double* ybin;               // kOutBinned: binned states (stride incy states)
+  long long incy;
+  int split;                  // rows kernel: warps per row (1, 2, 4, 8)
+  double* scratch;            // cols kernel: partial states
+  unsigned* tickets;          // cols kernel: one per column block, zero on entry
+};
+
+struct GemmArgs {
+  long long M, N, K;
+  const double* A;
+  long long sai, sak;         // op(A)_ik = A[i*sai + k*sak]
+  const double* B;
+  long long sbk, sbj;         // op(B)_kj = B[k*sbk + j*sbj]
+  double alpha, beta;
+  int mode;
+  double* C;                  // kOutValue
+  double* Cbin;               // kOutBinned
+  long long sci, scj;         // C_ij at offset i*sci + j*scj (values or states)
+};
+
+struct Blas23FoldOps {
+  cudaError_t (*gemv)(const GemvArgs& g, bool rows, dim3 grid, cudaStream_t s);
+  cudaError_t (*gemm)(const GemmArgs& g, cudaStream_t s, int* bm, int* bn);
+};
+extern const Blas23FoldOps blas23_fold2, blas23_fold3, blas23_fold4, blas23_fold5,
+    blas23_fold6, blas23_fold7, blas23_fold8;
+
 bool fold_supported(int fold);
 constexpr int kMaxFold = 8;
 

@@ -1,4 +1,5 @@
 // rb_runtime.cu -- host runtime: error channel, streams, workspaces, pointer classification.
+#include <cstdlib>
 #include <map>
 #include <memory>
 #include <utility>
@@ -92,12 +93,29 @@ bool Workspace::ensure_ring(size_t chunk) {
 
 bool Workspace::ensure_big(size_t bytes) {
   if (bytes <= big_bytes) return true;
+  // drain the stream first: kernels in flight may still read the old buffer
+  if (!cuda_ok(cudaStreamSynchronize(stream), "cudaStreamSynchronize")) return false;
   if (big) { cudaFree(big); big = nullptr; big_bytes = 0; }
   if (cudaMalloc(&big, bytes) != cudaSuccess) {
     set_error(RB_ERR_ALLOC, "workspace allocation failed");
     return false;
   }
   big_bytes = bytes;
+  return true;
+}
+
+bool Workspace::ensure_tickets(size_t n) {
+  if (n <= ntickets) return true;
+  // drain the stream first: kernels in flight may still use the old ticket array
+  if (!cuda_ok(cudaStreamSynchronize(stream), "cudaStreamSynchronize")) return false;
+  if (tickets) { cudaFree(tickets); tickets = nullptr; ntickets = 0; }
+  size_t want = n < 65536 ? 65536 : n;
+  if (cudaMalloc(&tickets, want * sizeof(unsigned)) != cudaSuccess) {
+    set_error(RB_ERR_ALLOC, "ticket allocation failed");
+    return false;
+  }
+  if (!cuda_ok(cudaMemset(tickets, 0, want * sizeof(unsigned)), "cudaMemset")) return false;
+  ntickets = want;
   return true;
 }
 
