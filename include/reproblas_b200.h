@@ -163,6 +163,34 @@ void binnedBLAS_dbdgemm(const int fold, const char Order, const char TransA, con
                         double_binned *C, const int ldc);
 
 /* ------------------------------------------------------------------------------------
+ * Reproducible dgemm on the tensor cores through int8 slices (no reference counterpart;
+ * the reference's dgemm is reproBLAS_rdgemm above).
+ * C <- conv(binned(beta*C) + sum over digit pairs of exact int32 products), where each
+ * operand is sliced after an FP64 per-row (A) / per-column (B) exponent extraction into
+ * `nslices` (2..8) signed 7-bit digits; digit pairs with p + q < nslices are multiplied on
+ * tcgen05 (kind::i8, exact int32 accumulation in TMEM) and recombined in binned FP64
+ * accumulators of the given fold (2..4). The result is bit-identical for any tile shape
+ * or launch order. It is not bit-identical to reproBLAS_rdgemm (different arithmetic):
+ * |C - exact| <= (nslices + 3) * K * 2^(e_i + f_j - 7*nslices) + 2 ulp, with 2^e_i and
+ * 2^f_j bounding row i of alpha*op(A) and column j of op(B).
+ * A, B, C must be device memory and finite (Inf/NaN operands: RB_ERR_UNSUPPORTED, C
+ * unchanged). alpha scales A before slicing, as in reproBLAS_rdgemm. Returns an RB_* code.
+ * ------------------------------------------------------------------------------------ */
+int rb_dgemm_int8(const int fold, const char Order, const char TransA, const char TransB,
+                  const int M, const int N, const int K, const double alpha, const double *A,
+                  const int lda, const double *B, const int ldb, const double beta, double *C,
+                  const int ldc, const int nslices);
+
+/* Test hook for rb_dgemm_int8 (row-major, no transposes, alpha 1, fold 3): device outputs
+ * raw[t][Mp][Np] = the int32 accumulators of digit-pair sums p + q = t (padded sizes
+ * Mp = M rounded up to 128, Np = N rounded up to 64), the digit slices
+ * as_out[p][Mp][Kp] / bs_out[q][Np][Kp] (Kp = K rounded up to 64, B transposed) and the
+ * exponents ea_out[M] / fb_out[N]. Any output may be NULL except raw. */
+int rb_dgemm_int8_inspect(const int M, const int N, const int K, const double *A,
+                          const double *B, const int nslices, int *raw, signed char *as_out,
+                          signed char *bs_out, int *ea_out, int *fb_out);
+
+/* ------------------------------------------------------------------------------------
  * B200 controls (no reference counterpart)
  * ------------------------------------------------------------------------------------ */
 

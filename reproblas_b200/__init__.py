@@ -64,6 +64,11 @@ SIGNATURES = {
                                   _c_int, _c_vp, _c_int, _c_vp, _c_int]),
     "binnedBLAS_dbdgemm": (None, [_c_int, _c_char, _c_char, _c_char, _c_int, _c_int, _c_int,
                                   _c_double, _c_vp, _c_int, _c_vp, _c_int, _c_vp, _c_int]),
+    "rb_dgemm_int8": (_c_int, [_c_int, _c_char, _c_char, _c_char, _c_int, _c_int, _c_int,
+                               _c_double, _c_vp, _c_int, _c_vp, _c_int, _c_double, _c_vp,
+                               _c_int, _c_int]),
+    "rb_dgemm_int8_inspect": (_c_int, [_c_int, _c_int, _c_int, _c_vp, _c_vp, _c_int, _c_vp,
+                                       _c_vp, _c_vp, _c_vp, _c_vp]),
     "rb_get_last_error": (_c_int, []),
     "rb_get_last_error_message": (ctypes.c_char_p, []),
     "rb_clear_error": (None, []),
