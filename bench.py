@@ -51,6 +51,12 @@ def parse():
     p.add_argument("--log2n", type=int, default=28)
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-secondary", action="store_true",
+                   help="skip the dgemm (plain vs int8-sliced) and dgemv measurements")
+    p.add_argument("--profile-kernel", choices=["int8", "plain_gemm", "gemv_n", "gemv_t"],
+                   help="only run that kernel `--steps` times on an n^3 (or n^2) case, for ncu")
+    p.add_argument("--profile-n", type=int, default=2048)
+    p.add_argument("--profile-slices", type=int, default=7)
     return p.parse_args()
 
 
@@ -317,6 +323,10 @@ def ours_arm(args, rank, world, local_rank):
                          "best of 3" % (args.log2n, threads),
                "bit_identical_to_gpu": bit_identical}
 
+    sec = None
+    if rank == 0 and world == 1 and not args.no_secondary:
+        sec = secondary(args)
+
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -344,6 +354,7 @@ def ours_arm(args, rank, world, local_rank):
                 "api": "reproBLAS_rddot(3, N, pinned host X, 1, pinned host Y, 1)"},
         "cpu_baseline": cpu,
         "result": res,
+        "secondary": sec,
     }
     traffic = os.path.join(ROOT, "profiles", "ddot_traffic.json")
     if os.path.exists(traffic):
@@ -355,8 +366,136 @@ def ours_arm(args, rank, world, local_rank):
     print(json.dumps(line))
 
 
+def _event_time(torch, fn, reps, warm=1):
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(reps):
+        fn()
+    e.record()
+    torch.cuda.synchronize()
+    return s.elapsed_time(e) / reps * 1e-3
+
+
+def int8_operands(rng, m, n):
+    """mantissas uniform in [1, 2), exponents uniform in [-20, 20], random signs"""
+    mant = rng.uniform(1.0, 2.0, (m, n))
+    ex = rng.integers(-20, 21, (m, n))
+    return np.ldexp(mant, ex) * rng.choice([-1.0, 1.0], (m, n))
+
+
+def secondary(args):
+    """dgemm TFLOP/s, plain binned vs int8-sliced (the second half of the headline metric),
+    and dgemv GB/s; rank 0 at N=1. Device-resident operands, CUDA-event timing."""
+    import torch
+    import reproblas_b200 as rb
+    from _ffi import port, ptr
+    out = {}
+    peak_bf16 = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak_bf16 = float(json.load(f)["bf16_tflops"])
+    except Exception:
+        peak_bf16 = 1590.0
+    rng = np.random.default_rng(8192)
+    # plain binned dgemm, BASELINE configuration: M=N=K=2048, uniform(-1,1), alpha 1.5, beta 0.5
+    n = 2048
+    A = torch.from_numpy(rng.uniform(-1, 1, (n, n))).cuda()
+    B = torch.from_numpy(rng.uniform(-1, 1, (n, n))).cuda()
+    C0 = torch.from_numpy(rng.uniform(-1, 1, (n, n))).cuda()
+    C = C0.clone()
+    t = _event_time(torch, lambda: rb.call("reproBLAS_rdgemm", 3, "r", "n", "n", n, n, n, 1.5, A, n, B, n,
+                                           0.5, C, n), 3)
+    out["dgemm_plain_2048"] = {"tflops": round(2 * n ** 3 / t / 1e12, 4), "ms": round(t * 1e3, 3),
+                               "bound": "fp64 pipe (binned deposit per product)"}
+    del A, B, C, C0
+    # 8192^3: plain binned vs int8-sliced on the int8 configuration's data
+    n = 8192
+    Ah = int8_operands(rng, n, n)
+    Bh = int8_operands(rng, n, n)
+    Ch = rng.uniform(-1, 1, (n, n))
+    A = torch.from_numpy(Ah).cuda(); B = torch.from_numpy(Bh).cuda()
+    C = torch.from_numpy(Ch).cuda()
+    t_plain = _event_time(torch, lambda: rb.call("reproBLAS_rdgemm", 3, "r", "n", "n", n, n, n, 1.5, A, n,
+                                                 B, n, 0.5, C, n), 1, warm=1)
+    out["dgemm_plain_8192"] = {"tflops": round(2 * n ** 3 / t_plain / 1e12, 4),
+                               "ms": round(t_plain * 1e3, 2)}
+    for S in (6, 7, 8):
+        C.copy_(torch.from_numpy(Ch))
+        t8 = _event_time(torch, lambda: rb.call("rb_dgemm_int8", 3, "r", "n", "n", n, n, n, 1.5, A, n, B,
+                                                n, 0.5, C, n, S), 3)
+        pairs = S * (S + 1) // 2
+        tops = 2.0 * pairs * n ** 3 / t8 / 1e12
+        rec = {"tflops_effective": round(2 * n ** 3 / t8 / 1e12, 3), "ms": round(t8 * 1e3, 3),
+               "slices": S, "digit_pairs": pairs, "int8_tops_issued": round(tops, 1),
+               "int8_peak_tops": round(2 * peak_bf16, 1),
+               "int8_frac": round(tops / (2 * peak_bf16), 4),
+               "speedup_vs_plain": round(t_plain / t8, 2)}
+        # error vs the exact host oracle on 4096 sampled entries, beside binned_dbbound
+        C.copy_(torch.from_numpy(Ch))
+        rb.call("rb_dgemm_int8", 3, "r", "n", "n", n, n, n, 1.5, A, n, B, n, 0.5, C, n, S)
+        got = C.cpu().numpy()
+        P = port()
+        srng = np.random.default_rng(S)
+        errs, ratios = [], []
+        for _ in range(4096):
+            i, j = int(srng.integers(0, n)), int(srng.integers(0, n))
+            a = np.ascontiguousarray(np.concatenate([Ah[i, :] * 1.5, [Ch[i, j] * 0.5]]))
+            b = np.ascontiguousarray(np.concatenate([Bh[:, j], [1.0]]))
+            ex = P.exact_dot(n + 1, ptr(a), 1, ptr(b), 1)
+            err = abs(got[i, j] - ex)
+            bound = P.dbbound(3, n + 1, float(np.max(np.abs(a * b))), ex)
+            errs.append(err / max(abs(ex), 1e-300))
+            ratios.append(err / bound)
+        rec["rel_err_max"] = float(np.max(errs))
+        rec["rel_err_mean"] = float(np.mean(errs))
+        rec["err_over_binned_bound_max"] = float(np.max(ratios))
+        rec["err_over_binned_bound_mean"] = float(np.mean(ratios))
+        out["dgemm_int8_8192_s%d" % S] = rec
+    del A, B, C
+    # dgemv 4096 x 4096, NoTrans and Trans
+    m = 4096
+    A = torch.from_numpy(rng.uniform(-1, 1, (m, m))).cuda()
+    x = torch.from_numpy(rng.uniform(-1, 1, m)).cuda()
+    y = torch.from_numpy(rng.uniform(-1, 1, m)).cuda()
+    for ta in "nt":
+        t = _event_time(torch, lambda: rb.call("reproBLAS_rdgemv", 3, "r", ta, m, m, 1.5, A, m, x, 1, 0.5,
+                                               y, 1), 20, warm=3)
+        byts = 8.0 * m * m + 8 * 3 * m
+        out["dgemv_4096_" + ta] = {"gbs": round(byts / t / 1e9, 1), "us": round(t * 1e6, 2)}
+    return out
+
+
+def profile_case(args):
+    """A small case of one kernel for ncu captures (prints nothing but a short note)."""
+    import torch
+    import reproblas_b200 as rb
+    rng = np.random.default_rng(1)
+    n = args.profile_n
+    A = torch.from_numpy(int8_operands(rng, n, n)).cuda()
+    B = torch.from_numpy(int8_operands(rng, n, n)).cuda()
+    C = torch.from_numpy(rng.uniform(-1, 1, (n, n))).cuda()
+    x = torch.from_numpy(rng.uniform(-1, 1, n)).cuda()
+    y = torch.from_numpy(rng.uniform(-1, 1, n)).cuda()
+    for _ in range(args.warmup + args.steps):
+        if args.profile_kernel == "int8":
+            rb.call("rb_dgemm_int8", 3, "r", "n", "n", n, n, n, 1.5, A, n, B, n, 0.5, C, n,
+                    args.profile_slices)
+        elif args.profile_kernel == "plain_gemm":
+            rb.call("reproBLAS_rdgemm", 3, "r", "n", "n", n, n, n, 1.5, A, n, B, n, 0.5, C, n)
+        else:
+            rb.call("reproBLAS_rdgemv", 3, "r", args.profile_kernel[-1], n, n, 1.5, A, n, x, 1, 0.5, y, 1)
+    torch.cuda.synchronize()
+    print("profile case done: %s n=%d" % (args.profile_kernel, n))
+
+
 def main():
     args = parse()
+    if args.profile_kernel:
+        profile_case(args)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
