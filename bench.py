@@ -386,6 +386,63 @@ def int8_operands(rng, m, n):
     return np.ldexp(mant, ex) * rng.choice([-1.0, 1.0], (m, n))
 
 
+def batched_case(torch, rb, rng):
+    """Batched ragged configuration: 10,000 ddot segments with log-uniform lengths (drawn as
+    floor(2^U(0,20)), then scaled so the total is ~2^28 elements, normal values) and 512
+    dgemm instances with m, n, k uniform over {16..256}, uniform(-1,1), fold 3; autotuned
+    schedule; one graph launch per step."""
+    import ctypes
+    nseg = 10000
+    lens = np.floor(np.exp2(rng.uniform(0, 20, nseg)))
+    lens = np.maximum(1, np.floor(lens * (2.0 ** 28 / lens.sum()))).astype(np.int32)
+    offs = np.concatenate([[0], np.cumsum(lens.astype(np.int64))[:-1]]).astype(np.int64)
+    total = int(lens.astype(np.int64).sum())
+    X = torch.from_numpy(rng.standard_normal(total)).cuda()
+    Y = torch.from_numpy(rng.standard_normal(total)).cuda()
+    res = torch.zeros(nseg, dtype=torch.float64, device="cuda")
+    ng = 512
+    inst = (rb.DgemmInstance * ng)()
+    keep = []
+    flops = 0.0
+    for g in range(ng):
+        m, n, k = (int(v) for v in rng.integers(16, 257, 3))
+        A = torch.from_numpy(rng.uniform(-1, 1, m * k)).cuda()
+        B = torch.from_numpy(rng.uniform(-1, 1, k * n)).cuda()
+        C = torch.from_numpy(rng.uniform(-1, 1, m * n)).cuda()
+        keep += [A, B, C]
+        d = inst[g]
+        d.order, d.transa, d.transb = b"r", b"n", b"n"
+        d.m, d.n, d.k, d.alpha, d.beta = m, n, k, 1.5, 0.5
+        d.A, d.lda, d.B, d.ldb, d.C, d.ldc = A.data_ptr(), k, B.data_ptr(), n, C.data_ptr(), n
+        flops += 2.0 * m * n * k
+    plan = rb.lib.rb_batch_plan_create(3, nseg, offs.ctypes.data, lens.ctypes.data, X.data_ptr(),
+                                       Y.data_ptr(), res.data_ptr(), None, ng, ctypes.addressof(inst))
+    rb.check()
+    t0 = time.perf_counter()
+    rb.call("rb_batch_plan_autotune", plan, 3)
+    tune_s = time.perf_counter() - t0
+    info = [ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong(), ctypes.c_longlong(),
+            ctypes.c_int(), ctypes.c_int(), ctypes.c_int()]
+    rb.lib.rb_batch_plan_info(plan, *[ctypes.byref(v) for v in info])
+    stream = torch.cuda.current_stream().cuda_stream
+    t = _event_time(torch, lambda: rb.call("rb_batch_plan_run", plan, stream), 5, warm=2)
+    # spot check: 64 segments equal the per-instance call
+    srng = np.random.default_rng(5)
+    got = res.cpu().numpy()
+    same = True
+    for i in srng.integers(0, nseg, 64):
+        o, l = int(offs[i]), int(lens[i])
+        same &= rb.call("reproBLAS_rddot", 3, l, X[o:], 1, Y[o:], 1) == got[i]
+    rb.lib.rb_batch_plan_destroy(plan)
+    return {"ms": round(t * 1e3, 3), "segments": nseg, "segment_elements": total,
+            "dgemm_instances": ng, "reduction_gbs": round(16.0 * total / t / 1e9, 1),
+            "gemm_tflops_if_alone": round(flops / t / 1e12, 3),
+            "schedule": {"tile": [info[0].value, info[1].value], "chunk": info[2].value,
+                         "small_max": info[3].value, "ctas_per_sm": info[4].value},
+            "autotune": {"tried": info[5].value, "rejected": info[6].value, "seconds": round(tune_s, 2)},
+            "spot_check_bit_identical": bool(same)}
+
+
 def secondary(args):
     """dgemm TFLOP/s, plain binned vs int8-sliced (the second half of the headline metric),
     and dgemv GB/s; rank 0 at N=1. Device-resident operands, CUDA-event timing."""
@@ -455,6 +512,7 @@ def secondary(args):
         rec["err_over_binned_bound_mean"] = float(np.mean(ratios))
         out["dgemm_int8_8192_s%d" % S] = rec
     del A, B, C
+    out["batched"] = batched_case(torch, rb, rng)
     # dgemv 4096 x 4096, NoTrans and Trans
     m = 4096
     A = torch.from_numpy(rng.uniform(-1, 1, (m, m))).cuda()

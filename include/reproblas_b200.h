@@ -191,6 +191,53 @@ int rb_dgemm_int8_inspect(const int M, const int N, const int K, const double *A
                           signed char *bs_out, int *ea_out, int *fb_out);
 
 /* ------------------------------------------------------------------------------------
+ * Batched ragged form (no reference counterpart as one call): many reproducible dot
+ * products / sums over segments of two device vectors and many small dgemm instances in
+ * ONE persistent launch, executed as a CUDA graph. Every segment result is bit-identical
+ * to reproBLAS_rddot (Y != NULL) or reproBLAS_rdsum (Y == NULL) on that segment -- or,
+ * with `states`, to binnedBLAS_dbddot / dbdsum accumulating into states[i] -- and every
+ * dgemm instance to reproBLAS_rdgemm on it (C updated in place).
+ * ------------------------------------------------------------------------------------ */
+typedef struct rb_batch_plan rb_batch_plan;
+
+typedef struct {
+  char order, transa, transb;    /* as reproBLAS_rdgemm */
+  int m, n, k;
+  double alpha;
+  const double *A;               /* device */
+  int lda;
+  const double *B;               /* device */
+  int ldb;
+  double beta;
+  double *C;                     /* device */
+  int ldc;
+} rb_dgemm_instance;
+
+/* Segment i is X[seg_offsets[i] .. + seg_lengths[i]) (and the same range of Y); X, Y,
+ * results[nseg] and states[nseg * 2 * fold] (optional) are device memory; the offset and
+ * length arrays and the instance array are read on the host at creation. fold in 2..4.
+ * Returns NULL on error (rb_get_last_error). */
+rb_batch_plan *rb_batch_plan_create(const int fold, const int nseg, const long long *seg_offsets,
+                                    const int *seg_lengths, const double *X, const double *Y,
+                                    double *results, double_binned *states, const int ngemm,
+                                    const rb_dgemm_instance *gemms);
+/* Tries every candidate schedule (gemm tile 16x16 / 32x32 / 32x64, long-segment chunk
+ * length, short-segment threshold, CTAs per SM) from the plan's original outputs,
+ * rejects any candidate whose output bits differ from the first candidate's, keeps the
+ * fastest over `reps` timed launches, and restores the outputs. Synchronises the device. */
+int rb_batch_plan_autotune(rb_batch_plan *plan, const int reps);
+/* Sets the schedule explicitly (tile 0: 16x16, 1: 32x32, 2: 32x64 with fold <= 3). */
+int rb_batch_plan_set_config(rb_batch_plan *plan, const int tile, const long long chunk,
+                             const long long small_max, const int ctas_per_sm);
+/* Enqueues one execution (one graph launch of the single persistent kernel) on `stream`.
+ * The first run after creation or a configuration change captures the graph. */
+int rb_batch_plan_run(rb_batch_plan *plan, void *stream);
+/* Chosen schedule and the autotuner's counts of candidates tried / rejected. */
+int rb_batch_plan_info(const rb_batch_plan *plan, int *tile_m, int *tile_n, long long *chunk,
+                       long long *small_max, int *ctas_per_sm, int *tried, int *rejected);
+void rb_batch_plan_destroy(rb_batch_plan *plan);
+
+/* ------------------------------------------------------------------------------------
  * B200 controls (no reference counterpart)
  * ------------------------------------------------------------------------------------ */
 

@@ -82,6 +82,25 @@ SIGNATURES = {
                                  _c_vp]),
 }
 
+class DgemmInstance(ctypes.Structure):
+    """rb_dgemm_instance (include/reproblas_b200.h)"""
+    _fields_ = [("order", ctypes.c_char), ("transa", ctypes.c_char), ("transb", ctypes.c_char),
+                ("m", ctypes.c_int), ("n", ctypes.c_int), ("k", ctypes.c_int),
+                ("alpha", ctypes.c_double), ("A", ctypes.c_void_p), ("lda", ctypes.c_int),
+                ("B", ctypes.c_void_p), ("ldb", ctypes.c_int), ("beta", ctypes.c_double),
+                ("C", ctypes.c_void_p), ("ldc", ctypes.c_int)]
+
+
+SIGNATURES.update({
+    "rb_batch_plan_create": (_c_vp, [_c_int, _c_int, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp,
+                                     _c_int, _c_vp]),
+    "rb_batch_plan_autotune": (_c_int, [_c_vp, _c_int]),
+    "rb_batch_plan_set_config": (_c_int, [_c_vp, _c_int, _c_ll, _c_ll, _c_int]),
+    "rb_batch_plan_run": (_c_int, [_c_vp, _c_vp]),
+    "rb_batch_plan_info": (_c_int, [_c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp, _c_vp]),
+    "rb_batch_plan_destroy": (None, [_c_vp]),
+})
+
 lib = ctypes.CDLL(LIB_PATH)
 for _name, (_res, _args) in SIGNATURES.items():
     if hasattr(lib, _name):

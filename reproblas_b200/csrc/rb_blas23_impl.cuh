@@ -213,15 +213,16 @@ struct GemmCfg {
   static constexpr int BK = 32;
 };
 
+// One BM x BN tile of C at (m0, n0), computed by the 256 threads of the calling CTA (the
+// caller must keep the whole CTA in step: the tile uses __syncthreads).
 template <int F, int TM, int TN>
-__global__ void __launch_bounds__(256) gemm_kernel(GemmArgs g) {
+__device__ __forceinline__ void gemm_tile(const GemmArgs& g, long long m0, long long n0) {
   using Cfg = GemmCfg<F, TM, TN>;
   constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK;
   __shared__ double As[BK][BM + 1];
   __shared__ double Bs[BK][BN + 1];
   const int tid = threadIdx.x;
   const int tx = tid % Cfg::TX, ty = tid / Cfg::TX;
-  const long long m0 = (long long)blockIdx.y * BM, n0 = (long long)blockIdx.x * BN;
 
   Acc<double, F> acc[TM][TN];
 #pragma unroll
@@ -295,6 +296,12 @@ __global__ void __launch_bounds__(256) gemm_kernel(GemmArgs g) {
         finish_entry<F>(acc[i][j], g.mode, g.C + off, g.beta, g.Cbin + off * 2 * F);
       }
     }
+}
+
+template <int F, int TM, int TN>
+__global__ void __launch_bounds__(256) gemm_kernel(GemmArgs g) {
+  using Cfg = GemmCfg<F, TM, TN>;
+  gemm_tile<F, TM, TN>(g, (long long)blockIdx.y * Cfg::BM, (long long)blockIdx.x * Cfg::BN);
 }
 
 template <int F>
