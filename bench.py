@@ -223,16 +223,10 @@ def ours_arm(args, rank, world, local_rank):
         Z.zero_()
         rb.call("binnedBLAS_dbddot", FOLD, n, X, 1, Y, 1, Z)
 
-    gathered = None
-    if world > 1:
-        gathered = torch.empty(world * 2 * FOLD, dtype=torch.float64, device="cuda")
-
     def combine():
-        # exchange the 48-byte per-rank states and merge them on every GPU
-        dist.all_gather_into_tensor(gathered, Z)
-        total = torch.zeros(2 * FOLD, dtype=torch.float64, device="cuda")
-        rb.call("rb_dbdbadd_states", FOLD, world, gathered, total)
-        return total
+        # exchange the 48-byte per-rank states over NCCL and merge them on every GPU
+        from reproblas_b200.distributed import allgather_merge
+        return allgather_merge(Z, FOLD)
 
     for _ in range(args.warmup):
         step()
