@@ -473,7 +473,7 @@ def secondary(args):
                                                  B, n, 0.5, C, n), 1, warm=1)
     out["dgemm_plain_8192"] = {"tflops": round(2 * n ** 3 / t_plain / 1e12, 4),
                                "ms": round(t_plain * 1e3, 2)}
-    for S in (6, 7, 8):
+    for S in (6, 7, 8, 10):
         C.copy_(torch.from_numpy(Ch))
         t8 = _event_time(torch, lambda: rb.call("rb_dgemm_int8", 3, "r", "n", "n", n, n, n, 1.5, A, n, B,
                                                 n, 0.5, C, n, S), 3)

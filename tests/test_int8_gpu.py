@@ -29,13 +29,13 @@ def rup(x, m):
     return (x + m - 1) // m * m
 
 
-@pytest.mark.parametrize("S", [2, 4, 7, 8])
+@pytest.mark.parametrize("S", [2, 3, 4, 7, 8, 9, 12])
 def test_raw_accumulators_exact(cuda, rb, S):
     rng = np.random.default_rng(S)
     M, N, K = 200, 100, 300
     A = baseline_operands(rng, M, K)
     B = baseline_operands(rng, K, N)
-    Mp, Np, Kp = rup(M, 128), rup(N, 64), rup(K, 64)
+    Mp, Np, Kp = rup(M, 128), rup(N, 64 if S <= 8 else 32), rup(K, 32)
     raw = cuda.zeros(S * Mp * Np, dtype=cuda.int32, device="cuda")
     As = cuda.zeros(S * Mp * Kp, dtype=cuda.int8, device="cuda")
     Bs = cuda.zeros(S * Np * Kp, dtype=cuda.int8, device="cuda")
@@ -43,8 +43,11 @@ def test_raw_accumulators_exact(cuda, rb, S):
     fb = cuda.zeros(N, dtype=cuda.int32, device="cuda")
     code = rb.call("rb_dgemm_int8_inspect", M, N, K, dev(cuda, A), dev(cuda, B), S, raw, As, Bs, ea, fb)
     assert code == 0
-    As = As.cpu().numpy().reshape(S, Mp, Kp).astype(np.int64)
-    Bs = Bs.cpu().numpy().reshape(S, Np, Kp).astype(np.int64)
+    # pre-tiled layout [Kp/16][S][rows/8][8][16] -> [S][rows][Kp]
+    As = As.cpu().numpy().reshape(Kp // 16, S, Mp // 8, 8, 16).transpose(1, 2, 3, 0, 4)
+    As = As.reshape(S, Mp, Kp).astype(np.int64)
+    Bs = Bs.cpu().numpy().reshape(Kp // 16, S, Np // 8, 8, 16).transpose(1, 2, 3, 0, 4)
+    Bs = Bs.reshape(S, Np, Kp).astype(np.int64)
     ea = ea.cpu().numpy()
     fb = fb.cpu().numpy()
     # digits reconstruct the operands
@@ -71,7 +74,7 @@ def exact_entries(port, A, B, C, alpha, beta, idx):
     return np.array(out)
 
 
-@pytest.mark.parametrize("S", [6, 7, 8])
+@pytest.mark.parametrize("S", [6, 7, 8, 10, 12])
 def test_error_vs_exact_oracle(cuda, rb, port, S):
     rng = np.random.default_rng(10 + S)
     M, N, K = 384, 320, 1000
@@ -93,9 +96,10 @@ def test_error_vs_exact_oracle(cuda, rb, port, S):
     assert np.all(err <= bound), np.max(err / bound)
 
 
-def test_bit_identical_across_decompositions(cuda, rb):
+@pytest.mark.parametrize("S", [7, 10])
+def test_bit_identical_across_decompositions(cuda, rb, S):
     rng = np.random.default_rng(77)
-    M, N, K, S = 256, 256, 512, 7
+    M, N, K = 256, 256, 512
     A = baseline_operands(rng, M, K)
     B = baseline_operands(rng, K, N)
     C = rng.uniform(-1, 1, (M, N))
