@@ -167,7 +167,7 @@ void binnedBLAS_dbdgemm(const int fold, const char Order, const char TransA, con
  * the reference's dgemm is reproBLAS_rdgemm above).
  * C <- conv(binned(beta*C) + sum over digit pairs of exact int32 products), where each
  * operand is sliced after an FP64 per-row (A) / per-column (B) exponent extraction into
- * `nslices` (2..8) signed 7-bit digits; digit pairs with p + q < nslices are multiplied on
+ * `nslices` (2..12) signed 7-bit digits; digit pairs with p + q < nslices are multiplied on
  * tcgen05 (kind::i8, exact int32 accumulation in TMEM) and recombined in binned FP64
  * accumulators of the given fold (2..4). The result is bit-identical for any tile shape
  * or launch order. It is not bit-identical to reproBLAS_rdgemm (different arithmetic):
