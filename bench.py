@@ -380,6 +380,39 @@ def int8_operands(rng, m, n):
     return np.ldexp(mant, ex) * rng.choice([-1.0, 1.0], (m, n))
 
 
+def blas1_sweep(torch, rb):
+    """Every BLAS1 reduction on HBM-resident inputs of 2^28 real elements (2^27 complex),
+    fold 3: GB/s of algorithmic traffic and the fraction of the measured HBM copy peak."""
+    peak, _ = peaks()
+    g = torch.Generator(device="cuda").manual_seed(3)
+    n = 1 << 28
+    x = torch.randn(n, dtype=torch.float64, device="cuda", generator=g)
+    y = torch.randn(n, dtype=torch.float64, device="cuda", generator=g)
+    xf, yf = x.float(), y.float()
+    z = torch.zeros(2 * FOLD, dtype=torch.float64, device="cuda")
+    zs = torch.zeros(2 * FOLD, dtype=torch.float32, device="cuda")
+    zc = torch.zeros(4 * FOLD, dtype=torch.float64, device="cuda")
+    zcf = torch.zeros(4 * FOLD, dtype=torch.float32, device="cuda")
+    nc = n // 2   # complex elements over the same buffers
+    cases = {
+        "dsum": (8.0 * n, lambda: rb.call("binnedBLAS_dbdsum", FOLD, n, x, 1, z)),
+        "ddot": (16.0 * n, lambda: rb.call("binnedBLAS_dbddot", FOLD, n, x, 1, y, 1, z)),
+        "dnrm2_ssq": (8.0 * n, lambda: rb.call("binnedBLAS_dbdssq", FOLD, n, x, 1, 0.0, z)),
+        "ssum": (4.0 * n, lambda: rb.call("binnedBLAS_sbssum", FOLD, n, xf, 1, zs)),
+        "sdot": (8.0 * n, lambda: rb.call("binnedBLAS_sbsdot", FOLD, n, xf, 1, yf, 1, zs)),
+        "zsum": (16.0 * nc, lambda: rb.call("binnedBLAS_zbzsum", FOLD, nc, x, 1, zc)),
+        "zdotc": (32.0 * nc, lambda: rb.call("binnedBLAS_zbzdotc", FOLD, nc, x, 1, y, 1, zc)),
+        "csum": (8.0 * (n // 2), lambda: rb.call("binnedBLAS_cbcsum", FOLD, n // 2, xf, 1, zcf)),
+    }
+    out = {}
+    for name, (byts, fn) in cases.items():
+        t = _event_time(torch, fn, 10, warm=3)
+        gbs = byts / t / 1e9
+        out[name] = {"gbs": round(gbs, 1), "frac_of_copy_peak": round(gbs / peak, 3),
+                     "us": round(t * 1e6, 1)}
+    return out
+
+
 def batched_case(torch, rb, rng):
     """Batched ragged configuration: 10,000 ddot segments with log-uniform lengths (drawn as
     floor(2^U(0,20)), then scaled so the total is ~2^28 elements, normal values) and 512
@@ -443,7 +476,7 @@ def secondary(args):
     import torch
     import reproblas_b200 as rb
     from _ffi import port, ptr
-    out = {}
+    out = {"blas1": blas1_sweep(torch, rb)}
     peak_bf16 = None
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:

@@ -101,8 +101,11 @@ bool run_gemv(const GemvReq& q) {
   size_t part_bytes = 0;
   DeviceInfo di;
   if (!device_info(&di)) return false;
+  // 16-byte loads when rows (and x for the row kernel) are 16-byte aligned
+  const bool a_al = (q.lda % 2) == 0;
+  const bool vec = nt ? (a_al && q.incX == 1) : (a_al && (nout % 2) == 0);
   if (!nt) {
-    col_blocks = (int)((nout + 255) / 256);
+    col_blocks = (int)((nout + (vec ? 511 : 255)) / (vec ? 512 : 256));
     long long target = (long long)di.sms * 4;
     long long ch = (target + col_blocks - 1) / col_blocks;
     long long maxch = (nred_eff + 15) / 16;
@@ -126,6 +129,7 @@ bool run_gemv(const GemvReq& q) {
   if (!ok) return false;
 
   GemvArgs g{};
+  g.vec = vec && ((uintptr_t)dA % 16) == 0 && (!nt || ((uintptr_t)dX % 16) == 0);
   g.A = dA;
   g.lda = q.lda;
   g.x = dX;
@@ -141,7 +145,7 @@ bool run_gemv(const GemvReq& q) {
   if (nt) {
     g.R = nout;
     g.C = nred_eff;
-    long long target_warps = (long long)di.sms * 32;
+    long long target_warps = (long long)di.sms * 16;   // a warp per row is enough in flight
     int S = 1;
     while (S < 8 && nout * S < target_warps) S *= 2;
     g.split = S;

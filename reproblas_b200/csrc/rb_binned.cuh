@@ -65,6 +65,11 @@ template <> struct BT<double> {
     int e = (int)(k >> 20);
     return e == 0 ? kMaxIndex : (2046 - e) / 40;
   }
+  // Smallest key whose index is below i: (2046 - e) / 40 < i  <=>  e >= 2047 - 40 i.
+  // Zero and subnormal keys (index 51) never are. 0 for the empty state (anything raises).
+  static __device__ __forceinline__ unsigned cap_of(int i) {
+    return i >= kMaxIndex + 1 ? 0u : (unsigned)(2047 - 40 * i) << 20;
+  }
   static __device__ __forceinline__ double compress(double x) { return __dmul_rn(x, 0x1p-14); }
   static __device__ __forceinline__ double half_expand(double m) { return __dmul_rn(m, 0x1p13); }
   static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
@@ -107,6 +112,11 @@ template <> struct BT<float> {
   static constexpr unsigned kInfKey = 0x7f800000u;
   static __device__ __forceinline__ unsigned key(float x) { return __float_as_uint(x) & 0x7fffffffu; }
   static __device__ __forceinline__ int index_of_key(unsigned k) { return index_of_abs(k); }
+  // Smallest key whose index is below i for normal magnitudes: e >= 255 - 13 i. Near the
+  // bottom (i >= 19) subnormal indices depend on the leading bit, so every key is checked.
+  static __device__ __forceinline__ unsigned cap_of(int i) {
+    return i >= 19 ? 0u : (unsigned)(255 - 13 * i) << 23;
+  }
   static __device__ __forceinline__ float compress(float x) { return __fmul_rn(x, 0x1p-12f); }
   static __device__ __forceinline__ float half_expand(float m) { return __fmul_rn(m, 0x1p11f); }
   static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
@@ -148,11 +158,18 @@ template <typename T, int F> struct Acc {
   int idx;        // bin index of pri[0], kEmpty if empty
   int deposits;   // deposits since the last renormalisation
   unsigned flags; // non-finite classes seen
+  unsigned cap;   // magnitude keys >= cap may need a coarser index (see BT::cap_of)
+
+  __device__ __forceinline__ void set_idx(int i) { idx = i; cap = B::cap_of(i); }
+  __device__ __forceinline__ void set_idx_from_pri() {
+    set_idx(pri[0] == T(0) ? kEmpty : B::mindex(pri[0]));
+  }
 
   __device__ __forceinline__ void zero() {
 #pragma unroll
     for (int i = 0; i < F; i++) { pri[i] = T(0); car[i] = T(0); }
     idx = kEmpty;
+    cap = 0u;
     deposits = 0;
     flags = 0;
   }
@@ -169,7 +186,7 @@ template <typename T, int F> struct Acc {
     }
 #pragma unroll
     for (int i = 0; i < F; i++) { pri[i] = p[i * inc]; car[i] = c[i * inc]; }
-    idx = (p0 == T(0)) ? kEmpty : B::mindex(p0);
+    set_idx((p0 == T(0)) ? kEmpty : B::mindex(p0));
   }
 
   __device__ __forceinline__ void store(T* p, T* c, int inc) const {
@@ -212,7 +229,7 @@ template <typename T, int F> struct Acc {
         car[i] = c;
       }
     }
-    idx = ni;
+    set_idx(ni);
   }
 
   // binned_dmddeposit's arithmetic (src/binned/dmddeposit.c:57-70), index != 0
@@ -246,8 +263,10 @@ template <typename T, int F> struct Acc {
   // index to that of the largest magnitude if needed (dmdupdate).
   __device__ __forceinline__ void prepare(unsigned amax_key, int n) {
     if (deposits + n > B::kEndurance) renorm();
-    int ni = B::index_of_key(amax_key);
-    if (ni < idx) raise_to(ni);
+    if (amax_key >= cap) {
+      const int ni = B::index_of_key(amax_key);
+      if (ni < idx) raise_to(ni);
+    }
     deposits += n;
   }
 
@@ -285,7 +304,7 @@ template <typename T, int F> struct Acc {
     if (idx == kEmpty) {
 #pragma unroll
       for (int i = 0; i < F; i++) { pri[i] = X.pri[i]; car[i] = X.car[i]; }
-      idx = X.idx;
+      set_idx(X.idx);
       deposits = 0;
       return;
     }
@@ -305,7 +324,7 @@ template <typename T, int F> struct Acc {
         pri[i] = p;
         car[i] = c;
       }
-      idx = X.idx;
+      set_idx(X.idx);
     } else {
       int sh = -shift;
 #pragma unroll
@@ -332,6 +351,7 @@ template <typename T, int F> struct Acc {
       o.car[i] = __shfl_xor_sync(0xffffffffu, car[i], mask);
     }
     o.idx = __shfl_xor_sync(0xffffffffu, idx, mask);
+    o.cap = 0u;   // not used by merge()
     o.flags = __shfl_xor_sync(0xffffffffu, flags, mask);
     o.deposits = 0;
     return o;

@@ -85,7 +85,7 @@ __device__ __forceinline__ void rescale(Acc<double, F>& a, double x, double scal
       }
     }
   }
-  a.idx = BT<double>::mindex(a.pri[0]);
+  a.set_idx(BT<double>::mindex(a.pri[0]));
 }
 
 // binned_dmdmaddsq (src/binned/dmdmaddsq.c:26-41): Y(scaleY) += X(scaleX)
@@ -191,7 +191,7 @@ struct Red1 {
     for (int i = 0; i < F; i++) { a.pri[i] = ldrec<G>(r + i); a.car[i] = ldrec<G>(r + F + i); }
     a.flags = (unsigned)BT<T>::bits(ldrec<G>(r + 2 * F));
     scl = (double)ldrec<G>(r + 2 * F + 1);
-    a.idx = (a.pri[0] == T(0)) ? kEmpty : BT<T>::mindex(a.pri[0]);
+    a.set_idx_from_pri();
     a.deposits = 0;
   }
 };
@@ -397,8 +397,8 @@ struct RedC {
     }
     re.flags = (unsigned)BT<T>::bits(ldrec<G>(r + 2 * F));
     im.flags = (unsigned)BT<T>::bits(ldrec<G>(r + 4 * F + 1));
-    re.idx = (re.pri[0] == T(0)) ? kEmpty : BT<T>::mindex(re.pri[0]);
-    im.idx = (im.pri[0] == T(0)) ? kEmpty : BT<T>::mindex(im.pri[0]);
+    re.set_idx_from_pri();
+    im.set_idx_from_pri();
     re.deposits = im.deposits = 0;
   }
 };
@@ -417,7 +417,7 @@ template <typename T, int F, int OP>
 __global__ void __launch_bounds__(256)
 blasc_kernel(Blas1Args args) {
   constexpr int REC = 4 * F + 2;
-  constexpr int K = 4;   // complex elements per thread per step
+  constexpr int K = OP == kOpCSum ? 8 : 4;   // complex elements per thread per step
   __shared__ T smem[32 * REC];
   using B = BT<T>;
 

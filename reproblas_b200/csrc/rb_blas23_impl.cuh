@@ -49,13 +49,38 @@ __device__ __forceinline__ void finish_entry(Acc<double, F>& a, int mode, double
   }
 }
 
+__device__ __forceinline__ void ld2(const double* p, double& a, double& b) {
+  double2 v = __ldg((const double2*)p);
+  a = v.x;
+  b = v.y;
+}
+
+// Merge `count` records (pri F, car F, flags) at `rec` (shared memory) into `t`.
+template <int F>
+__device__ __forceinline__ void merge_records(Acc<double, F>& t, const double* rec, int count) {
+  constexpr int REC = 2 * F + 2;
+  for (int p = 0; p < count; p++) {
+    const double* r = rec + p * REC;
+    Acc<double, F> o;
+    o.zero();
+#pragma unroll
+    for (int i = 0; i < F; i++) { o.pri[i] = r[i]; o.car[i] = r[F + i]; }
+    o.flags = (unsigned)__double_as_longlong(r[2 * F]);
+    o.set_idx_from_pri();
+    t.merge(o);
+  }
+}
+
 // ---------------------------------------------------------------------------------------
 // gemv, reduction along contiguous rows: out_r = sum_c A[r*lda + c] * bx_c, r < R, c < C.
-// S warps share a row (S = 1, 2, 4, 8); a CTA of 8 warps covers 8/S rows.
+// S warps share a row (S = 1, 2, 4, 8); a CTA of 8 warps covers 8/S rows. With g.vec (row
+// starts and x 16-byte aligned, incx 1) lanes read 16-byte pairs: 512 contiguous bytes per
+// warp load; the row is cut into chunks of a multiple of 8 elements so they stay aligned.
 // ---------------------------------------------------------------------------------------
 template <int F>
 __global__ void __launch_bounds__(256) gemv_rows_kernel(GemvArgs g) {
-  __shared__ double smem[8 * (2 * F + 2)];
+  constexpr int REC = 2 * F + 2;
+  __shared__ double smem[8 * REC];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int S = g.split;
   const int rows_per_cta = 8 / S;
@@ -65,32 +90,62 @@ __global__ void __launch_bounds__(256) gemv_rows_kernel(GemvArgs g) {
   a.zero();
   if (r < g.R) {
     const double* row = g.A + r * g.lda;
-    const long long chunk = (g.C + S - 1) / S;
-    const long long c0 = part * chunk;
+    const long long chunk = ((g.C + S - 1) / S + 7) / 8 * 8;
+    const long long c0 = part * chunk < g.C ? part * chunk : g.C;
     const long long c1 = c0 + chunk < g.C ? c0 + chunk : g.C;
-    constexpr int K = 4;
+    if (g.vec) {
+      const long long npair = (c1 - c0) / 2;
+      constexpr int K = 4;
 #pragma unroll 1
-    for (long long b = c0 + lane; b < c1; b += 32 * K) {
-      double v[K];
-      int nv = 0;
+      for (long long pb = lane; pb < npair; pb += 32 * K) {
+        double v[2 * K];
+        int nv = 0;
 #pragma unroll
-      for (int k = 0; k < K; k++) {
-        long long c = b + 32 * k;
-        v[k] = 0.0;
-        if (c < c1) {
-          double xv = __ldg(g.x + c * g.incx);
-          if (g.alpha != 1.0) xv = __dmul_rn(xv, g.alpha);
-          v[k] = __dmul_rn(__ldg(row + c), xv);
-          nv = k + 1;
+        for (int k = 0; k < K; k++) {
+          const long long pi = pb + 32 * k;
+          v[2 * k] = v[2 * k + 1] = 0.0;
+          if (pi < npair) {
+            double a0, a1, x0, x1;
+            ld2(row + c0 + 2 * pi, a0, a1);
+            ld2(g.x + c0 + 2 * pi, x0, x1);
+            if (g.alpha != 1.0) { x0 = __dmul_rn(x0, g.alpha); x1 = __dmul_rn(x1, g.alpha); }
+            v[2 * k] = __dmul_rn(a0, x0);
+            v[2 * k + 1] = __dmul_rn(a1, x1);
+            nv = 2 * k + 2;
+          }
         }
+        a.template tile<2 * K>(v, nv);
       }
-      a.template tile<K>(v, nv);
+      if (((c1 - c0) & 1) && lane == 0) {
+        double xv = __ldg(g.x + (c1 - 1));
+        if (g.alpha != 1.0) xv = __dmul_rn(xv, g.alpha);
+        double v[1] = {__dmul_rn(__ldg(row + (c1 - 1)), xv)};
+        a.template tile<1>(v, 1);
+      }
+    } else {
+      constexpr int K = 4;
+#pragma unroll 1
+      for (long long b = c0 + lane; b < c1; b += 32 * K) {
+        double v[K];
+        int nv = 0;
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+          long long c = b + 32 * k;
+          v[k] = 0.0;
+          if (c < c1) {
+            double xv = __ldg(g.x + c * g.incx);
+            if (g.alpha != 1.0) xv = __dmul_rn(xv, g.alpha);
+            v[k] = __dmul_rn(__ldg(row + c), xv);
+            nv = k + 1;
+          }
+        }
+        a.template tile<K>(v, nv);
+      }
     }
   }
   a.renorm();
 #pragma unroll 1
   for (int m = 16; m; m >>= 1) a.merge(a.shfl_xor(m));
-  constexpr int REC = 2 * F + 2;
   if (lane == 0) {
     double* rec = smem + warp * REC;
 #pragma unroll
@@ -103,67 +158,72 @@ __global__ void __launch_bounds__(256) gemv_rows_kernel(GemvArgs g) {
     if (rr < g.R) {
       Acc<double, F> t;
       t.zero();
-      for (int p = 0; p < S; p++) {
-        const double* rec = smem + (threadIdx.x * S + p) * REC;
-        Acc<double, F> o;
-        o.zero();
-#pragma unroll
-        for (int i = 0; i < F; i++) { o.pri[i] = rec[i]; o.car[i] = rec[F + i]; }
-        o.flags = (unsigned)__double_as_longlong(rec[2 * F]);
-        o.idx = o.pri[0] == 0.0 ? kEmpty : BT<double>::mindex(o.pri[0]);
-        t.merge(o);
-      }
-      finish_entry<F>(t, g.mode, g.y + rr * g.incy, g.beta,
-                      g.ybin + rr * g.incy * 2 * F);
+      merge_records<F>(t, smem + threadIdx.x * S * REC, S);
+      finish_entry<F>(t, g.mode, g.y + rr * g.incy, g.beta, g.ybin + rr * g.incy * 2 * F);
     }
   }
 }
 
 // ---------------------------------------------------------------------------------------
 // gemv, reduction along strided columns: out_c = sum_r A[r*lda + c] * bx_r, c < C, r < R.
-// grid = (column blocks of 256, row chunks). Each thread owns one column of one chunk;
-// partial states go to scratch (structure of arrays), and the last chunk-CTA to arrive for
-// a column block merges them.
+// grid = (column blocks of 256 * W, row chunks), W = 2 columns per thread with g.vec (A and
+// lda 16-byte aligned; one 16-byte load per row), else 1. Each thread owns W columns of one
+// chunk; partial states go to scratch (structure of arrays) and the last chunk-CTA to arrive
+// for a column block merges them.
 // ---------------------------------------------------------------------------------------
-template <int F>
-__global__ void __launch_bounds__(256) gemv_cols_kernel(GemvArgs g) {
-  constexpr int NF = 2 * F + 1;   // pri, car, flags
-  const long long c = (long long)blockIdx.x * 256 + threadIdx.x;
+template <int F, int W>
+__device__ __forceinline__ void gemv_cols_body(const GemvArgs& g) {
+  const long long cbase = ((long long)blockIdx.x * 256 + threadIdx.x) * W;
   const int chunk = blockIdx.y, nchunks = gridDim.y;
   const long long rows_per = (g.R + nchunks - 1) / nchunks;
   const long long r0 = (long long)chunk * rows_per;
   const long long r1 = r0 + rows_per < g.R ? r0 + rows_per : g.R;
-  Acc<double, F> a;
-  a.zero();
-  if (c < g.C) {
+  const long long stride = (long long)nchunks * g.C;
+  Acc<double, F> a[W];
+#pragma unroll
+  for (int w = 0; w < W; w++) a[w].zero();
+  if (cbase < g.C) {
     constexpr int K = 4;
 #pragma unroll 1
     for (long long b = r0; b < r1; b += K) {
-      double v[K];
+      double v[W][K];
       int nv = 0;
 #pragma unroll
       for (int k = 0; k < K; k++) {
-        long long r = b + k;
-        v[k] = 0.0;
+        const long long r = b + k;
+#pragma unroll
+        for (int w = 0; w < W; w++) v[w][k] = 0.0;
         if (r < r1) {
           double xv = __ldg(g.x + r * g.incx);
           if (g.alpha != 1.0) xv = __dmul_rn(xv, g.alpha);
-          v[k] = __dmul_rn(__ldg(g.A + r * g.lda + c), xv);
+          if constexpr (W == 2) {
+            double a0, a1;
+            ld2(g.A + r * g.lda + cbase, a0, a1);
+            v[0][k] = __dmul_rn(a0, xv);
+            v[1][k] = __dmul_rn(a1, xv);
+          } else {
+            v[0][k] = __dmul_rn(__ldg(g.A + r * g.lda + cbase), xv);
+          }
           nv = k + 1;
         }
       }
-      a.template tile<K>(v, nv);
-    }
-    a.renorm();
-    // scratch layout: field f, chunk, column  -> coalesced across the warp
-    double* s = g.scratch;
-    const long long stride = (long long)nchunks * g.C;
 #pragma unroll
-    for (int i = 0; i < F; i++) {
-      s[(long long)i * stride + (long long)chunk * g.C + c] = a.pri[i];
-      s[(long long)(F + i) * stride + (long long)chunk * g.C + c] = a.car[i];
+      for (int w = 0; w < W; w++) a[w].template tile<K>(v[w], nv);
     }
-    s[(long long)(2 * F) * stride + (long long)chunk * g.C + c] = __longlong_as_double((long long)a.flags);
+#pragma unroll
+    for (int w = 0; w < W; w++) {
+      const long long c = cbase + w;
+      if (c < g.C) {
+        a[w].renorm();
+        double* s = g.scratch;
+#pragma unroll
+        for (int i = 0; i < F; i++) {
+          s[(long long)i * stride + (long long)chunk * g.C + c] = a[w].pri[i];
+          s[(long long)(F + i) * stride + (long long)chunk * g.C + c] = a[w].car[i];
+        }
+        s[(long long)(2 * F) * stride + (long long)chunk * g.C + c] = __longlong_as_double((long long)a[w].flags);
+      }
+    }
   }
   // last chunk-CTA of this column block merges
   __shared__ unsigned s_last;
@@ -176,27 +236,48 @@ __global__ void __launch_bounds__(256) gemv_cols_kernel(GemvArgs g) {
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  if (c < g.C) {
-    const double* s = g.scratch;
-    const long long stride = (long long)nchunks * g.C;
-    Acc<double, F> t;
-    t.zero();
-    for (int ch = 0; ch < nchunks; ch++) {
-      Acc<double, F> o;
-      o.zero();
 #pragma unroll
-      for (int i = 0; i < F; i++) {
-        o.pri[i] = __ldcg(s + (long long)i * stride + (long long)ch * g.C + c);
-        o.car[i] = __ldcg(s + (long long)(F + i) * stride + (long long)ch * g.C + c);
+  for (int w = 0; w < W; w++) {
+    const long long c = cbase + w;
+    if (c < g.C) {
+      const double* s = g.scratch;
+      Acc<double, F> t;
+      t.zero();
+      // records are fetched 4 chunks at a time so their L2 latencies overlap
+      constexpr int PB = 4;
+#pragma unroll 1
+      for (int ch0 = 0; ch0 < nchunks; ch0 += PB) {
+        Acc<double, F> o[PB];
+#pragma unroll
+        for (int j = 0; j < PB; j++) {
+          o[j].zero();
+          const int ch = ch0 + j;
+          if (ch < nchunks) {
+#pragma unroll
+            for (int i = 0; i < F; i++) {
+              o[j].pri[i] = __ldcg(s + (long long)i * stride + (long long)ch * g.C + c);
+              o[j].car[i] = __ldcg(s + (long long)(F + i) * stride + (long long)ch * g.C + c);
+            }
+            o[j].flags = (unsigned)__double_as_longlong(
+                __ldcg(s + (long long)(2 * F) * stride + (long long)ch * g.C + c));
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < PB; j++) {
+          o[j].set_idx_from_pri();
+          t.merge(o[j]);
+        }
       }
-      o.flags = (unsigned)__double_as_longlong(__ldcg(s + (long long)(2 * F) * stride + (long long)ch * g.C + c));
-      o.idx = o.pri[0] == 0.0 ? kEmpty : BT<double>::mindex(o.pri[0]);
-      t.merge(o);
+      finish_entry<F>(t, g.mode, g.y + c * g.incy, g.beta, g.ybin + c * g.incy * 2 * F);
     }
-    finish_entry<F>(t, g.mode, g.y + c * g.incy, g.beta, g.ybin + c * g.incy * 2 * F);
   }
   if (threadIdx.x == 0) g.tickets[blockIdx.x] = 0u;
-  (void)NF;
+}
+
+template <int F>
+__global__ void __launch_bounds__(256) gemv_cols_kernel(GemvArgs g) {
+  if (g.vec) gemv_cols_body<F, 2>(g);
+  else gemv_cols_body<F, 1>(g);
 }
 
 // ---------------------------------------------------------------------------------------
