@@ -540,16 +540,28 @@ def secondary(args):
         out["dgemm_int8_8192_s%d" % S] = rec
     del A, B, C
     out["batched"] = batched_case(torch, rb, rng)
-    # dgemv 4096 x 4096, NoTrans and Trans
-    m = 4096
-    A = torch.from_numpy(rng.uniform(-1, 1, (m, m))).cuda()
-    x = torch.from_numpy(rng.uniform(-1, 1, m)).cuda()
-    y = torch.from_numpy(rng.uniform(-1, 1, m)).cuda()
-    for ta in "nt":
-        t = _event_time(torch, lambda: rb.call("reproBLAS_rdgemv", 3, "r", ta, m, m, 1.5, A, m, x, 1, 0.5,
-                                               y, 1), 20, warm=3)
-        byts = 8.0 * m * m + 8 * 3 * m
-        out["dgemv_4096_" + ta] = {"gbs": round(byts / t / 1e9, 1), "us": round(t * 1e6, 2)}
+    # dgemv, NoTrans (row reduction) and Trans (column reduction), row-major A: 4096^2
+    # (134 MB, about L2's size: launch and host-call latency show) and 16384^2 (2.1 GB).
+    # "us" is CUDA-event time per call over back-to-back calls, "host_us" the host time of
+    # one call (the API call returns after enqueueing, so us ~ host_us means host-bound).
+    for m in (4096, 16384):
+        A = torch.from_numpy(rng.uniform(-1, 1, (m, m))).cuda()
+        x = torch.from_numpy(rng.uniform(-1, 1, m)).cuda()
+        y = torch.from_numpy(rng.uniform(-1, 1, m)).cuda()
+        for ta in "nt":
+            call = lambda: rb.call("reproBLAS_rdgemv", 3, "r", ta, m, m, 1.5, A, m, x, 1, 0.5, y, 1)
+            reps = 20 if m == 4096 else 5
+            t = _event_time(torch, call, reps, warm=3)
+            torch.cuda.synchronize()
+            h0 = time.perf_counter()
+            call()
+            h1 = time.perf_counter()
+            torch.cuda.synchronize()
+            byts = 8.0 * m * m + 8 * 3 * m
+            out["dgemv_%d_%s" % (m, ta)] = {"gbs": round(byts / t / 1e9, 1), "us": round(t * 1e6, 2),
+                                            "host_us": round((h1 - h0) * 1e6, 1),
+                                            "frac_of_copy_peak": round(byts / t / 1e9 / peaks()[0], 3)}
+        del A, x, y
     return out
 
 

@@ -104,14 +104,35 @@ bool run_gemv(const GemvReq& q) {
   // 16-byte loads when rows (and x for the row kernel) are 16-byte aligned
   const bool a_al = (q.lda % 2) == 0;
   const bool vec = nt ? (a_al && q.incX == 1) : (a_al && (nout % 2) == 0);
+  int groups = 1;
   if (!nt) {
-    col_blocks = (int)((nout + (vec ? 511 : 255)) / (vec ? 512 : 256));
-    long long target = (long long)di.sms * 4;
-    long long ch = (target + col_blocks - 1) / col_blocks;
-    long long maxch = (nred_eff + 15) / 16;
-    if (ch > maxch) ch = maxch;
-    if (ch < 1) ch = 1;
-    nchunks = (int)ch;
+    // Column kernel shape: G row groups per CTA, T = 256/G threads per group, W columns per
+    // thread. Cost model in units of one row per thread: the streaming part (waves of CTAs
+    // times rows per thread, plus the in-CTA tree merge) and the serial merge of the chunk
+    // partials in the last CTA of each column block (about 4 units per merge).
+    const long long W = vec ? 2 : 1;
+    const long long slots = (long long)di.sms * 3;
+    long long best = -1;
+    for (int G = 1; G <= 8; G *= 2) {
+      const long long cols = (256 / G) * W;
+      const long long cb = (nout + cols - 1) / cols;
+      const long long maxch = (nred_eff + 8 * G - 1) / (8 * G);   // >= 8 rows per group
+      const long long lg = G == 1 ? 0 : G == 2 ? 1 : G == 4 ? 2 : 3;
+      // chunks: fill the slots exactly once (floor) or just over (ceil)
+      for (long long ch : {slots / cb, (slots + cb - 1) / cb}) {
+        if (ch > maxch) ch = maxch;
+        if (ch < 1) ch = 1;
+        const long long rpt = ((nred_eff + ch - 1) / ch + G - 1) / G;
+        const long long waves = (cb * ch + slots - 1) / slots;
+        const long long cost = waves * (rpt + 8 * lg) + 4 * ((ch + G - 1) / G + 2 * lg);
+        if (best < 0 || cost < best) {
+          best = cost;
+          groups = G;
+          col_blocks = (int)cb;
+          nchunks = (int)ch;
+        }
+      }
+    }
     part_bytes = (size_t)nchunks * nout * (2 * q.fold + 1) * 8;
     if (!w->ensure_tickets((size_t)col_blocks)) return false;
   }
@@ -155,7 +176,7 @@ bool run_gemv(const GemvReq& q) {
   } else {
     g.C = nout;
     g.R = nred_eff;
-    g.split = 1;
+    g.split = groups;
     g.scratch = part;
     g.tickets = w->tickets;
     dim3 grid((unsigned)col_blocks, (unsigned)nchunks);

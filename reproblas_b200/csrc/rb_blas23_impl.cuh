@@ -166,14 +166,58 @@ __global__ void __launch_bounds__(256) gemv_rows_kernel(GemvArgs g) {
 
 // ---------------------------------------------------------------------------------------
 // gemv, reduction along strided columns: out_c = sum_r A[r*lda + c] * bx_r, c < C, r < R.
-// grid = (column blocks of 256 * W, row chunks), W = 2 columns per thread with g.vec (A and
-// lda 16-byte aligned; one 16-byte load per row), else 1. Each thread owns W columns of one
-// chunk; partial states go to scratch (structure of arrays) and the last chunk-CTA to arrive
-// for a column block merges them.
+// A CTA of 256 threads is G = g.split row groups (1, 2, 4, 8) of T = 256/G threads; thread
+// t of a group owns W columns (W = 2 with g.vec, A and lda 16-byte aligned: one 16-byte load
+// per row; else 1), so a CTA covers T*W columns and a warp reads 32*W contiguous doubles of
+// a row. grid = (column blocks, row chunks); inside a chunk, group q takes rows q, q+G, ...
+// The groups' states are merged through shared memory, group 0 writes the chunk's partial
+// state to scratch (structure of arrays), and the last chunk-CTA to arrive for a column
+// block merges the partials (group q takes chunks q, q+G, ...; then the groups merge once
+// more) and finishes the entries. More groups mean narrower column blocks, more of them and
+// fewer chunks, which shortens that final serial merge.
 // ---------------------------------------------------------------------------------------
+
+// Tree merge of the G row groups' states (each renormalised) through shared memory laid out
+// as sm[i * 256 + thread], i < 2F+1; group 0 ends with the merged state. Every thread of the
+// CTA must call it.
+template <int F>
+__device__ __forceinline__ void merge_row_groups(Acc<double, F>& a, double* sm, int grp, int t,
+                                                 int G, int T) {
+#pragma unroll 1
+  for (int s = 1; s < G; s <<= 1) {
+    const int m = grp & (2 * s - 1);
+    if (m == s) {
+#pragma unroll
+      for (int i = 0; i < F; i++) {
+        sm[i * 256 + threadIdx.x] = a.pri[i];
+        sm[(F + i) * 256 + threadIdx.x] = a.car[i];
+      }
+      sm[2 * F * 256 + threadIdx.x] = __longlong_as_double((long long)a.flags);
+    }
+    __syncthreads();
+    if (m == 0) {
+      const int src = (grp + s) * T + t;
+      Acc<double, F> o;
+      o.zero();
+#pragma unroll
+      for (int i = 0; i < F; i++) {
+        o.pri[i] = sm[i * 256 + src];
+        o.car[i] = sm[(F + i) * 256 + src];
+      }
+      o.flags = (unsigned)__double_as_longlong(sm[2 * F * 256 + src]);
+      o.set_idx_from_pri();
+      a.merge(o);
+    }
+    __syncthreads();
+  }
+}
+
 template <int F, int W>
-__device__ __forceinline__ void gemv_cols_body(const GemvArgs& g) {
-  const long long cbase = ((long long)blockIdx.x * 256 + threadIdx.x) * W;
+__device__ __forceinline__ void gemv_cols_body(const GemvArgs& g, double* sm) {
+  const int G = g.split, T = 256 / G;
+  const int lgT = __ffs(T) - 1;
+  const int grp = threadIdx.x >> lgT, t = threadIdx.x & (T - 1);
+  const long long cbase = ((long long)blockIdx.x * T + t) * W;
   const int chunk = blockIdx.y, nchunks = gridDim.y;
   const long long rows_per = (g.R + nchunks - 1) / nchunks;
   const long long r0 = (long long)chunk * rows_per;
@@ -185,12 +229,12 @@ __device__ __forceinline__ void gemv_cols_body(const GemvArgs& g) {
   if (cbase < g.C) {
     constexpr int K = 4;
 #pragma unroll 1
-    for (long long b = r0; b < r1; b += K) {
+    for (long long b = r0 + grp; b < r1; b += (long long)G * K) {
       double v[W][K];
       int nv = 0;
 #pragma unroll
       for (int k = 0; k < K; k++) {
-        const long long r = b + k;
+        const long long r = b + (long long)k * G;
 #pragma unroll
         for (int w = 0; w < W; w++) v[w][k] = 0.0;
         if (r < r1) {
@@ -210,18 +254,24 @@ __device__ __forceinline__ void gemv_cols_body(const GemvArgs& g) {
 #pragma unroll
       for (int w = 0; w < W; w++) a[w].template tile<K>(v[w], nv);
     }
+  }
+#pragma unroll
+  for (int w = 0; w < W; w++) {
+    a[w].renorm();
+    merge_row_groups<F>(a[w], sm, grp, t, G, T);
+  }
+  if (grp == 0) {
 #pragma unroll
     for (int w = 0; w < W; w++) {
       const long long c = cbase + w;
       if (c < g.C) {
-        a[w].renorm();
-        double* s = g.scratch;
+        double* s = g.scratch + (long long)chunk * g.C + c;
 #pragma unroll
         for (int i = 0; i < F; i++) {
-          s[(long long)i * stride + (long long)chunk * g.C + c] = a[w].pri[i];
-          s[(long long)(F + i) * stride + (long long)chunk * g.C + c] = a[w].car[i];
+          s[(long long)i * stride] = a[w].pri[i];
+          s[(long long)(F + i) * stride] = a[w].car[i];
         }
-        s[(long long)(2 * F) * stride + (long long)chunk * g.C + c] = __longlong_as_double((long long)a[w].flags);
+        s[(long long)(2 * F) * stride] = __longlong_as_double((long long)a[w].flags);
       }
     }
   }
@@ -230,54 +280,53 @@ __device__ __forceinline__ void gemv_cols_body(const GemvArgs& g) {
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
-    unsigned t = atomicAdd(g.tickets + blockIdx.x, 1u);
-    s_last = (t == (unsigned)nchunks - 1) ? 1u : 0u;
+    unsigned tk = atomicAdd(g.tickets + blockIdx.x, 1u);
+    s_last = (tk == (unsigned)nchunks - 1) ? 1u : 0u;
   }
   __syncthreads();
   if (!s_last) return;
   __threadfence();
 #pragma unroll
-  for (int w = 0; w < W; w++) {
-    const long long c = cbase + w;
-    if (c < g.C) {
-      const double* s = g.scratch;
-      Acc<double, F> t;
-      t.zero();
-      // records are fetched 4 chunks at a time so their L2 latencies overlap
-      constexpr int PB = 4;
+  for (int w = 0; w < W; w++) a[w].zero();
+  if (cbase < g.C) {
 #pragma unroll 1
-      for (int ch0 = 0; ch0 < nchunks; ch0 += PB) {
-        Acc<double, F> o[PB];
+    for (int ch = grp; ch < nchunks; ch += G) {
 #pragma unroll
-        for (int j = 0; j < PB; j++) {
-          o[j].zero();
-          const int ch = ch0 + j;
-          if (ch < nchunks) {
+      for (int w = 0; w < W; w++) {
+        const long long c = cbase + w;
+        if (c < g.C) {
+          const double* s = g.scratch + (long long)ch * g.C + c;
+          Acc<double, F> o;
+          o.zero();
 #pragma unroll
-            for (int i = 0; i < F; i++) {
-              o[j].pri[i] = __ldcg(s + (long long)i * stride + (long long)ch * g.C + c);
-              o[j].car[i] = __ldcg(s + (long long)(F + i) * stride + (long long)ch * g.C + c);
-            }
-            o[j].flags = (unsigned)__double_as_longlong(
-                __ldcg(s + (long long)(2 * F) * stride + (long long)ch * g.C + c));
+          for (int i = 0; i < F; i++) {
+            o.pri[i] = __ldcg(s + (long long)i * stride);
+            o.car[i] = __ldcg(s + (long long)(F + i) * stride);
           }
-        }
-#pragma unroll
-        for (int j = 0; j < PB; j++) {
-          o[j].set_idx_from_pri();
-          t.merge(o[j]);
+          o.flags = (unsigned)__double_as_longlong(__ldcg(s + (long long)(2 * F) * stride));
+          o.set_idx_from_pri();
+          a[w].merge(o);
         }
       }
-      finish_entry<F>(t, g.mode, g.y + c * g.incy, g.beta, g.ybin + c * g.incy * 2 * F);
+    }
+  }
+#pragma unroll
+  for (int w = 0; w < W; w++) merge_row_groups<F>(a[w], sm, grp, t, G, T);
+  if (grp == 0) {
+#pragma unroll
+    for (int w = 0; w < W; w++) {
+      const long long c = cbase + w;
+      if (c < g.C) finish_entry<F>(a[w], g.mode, g.y + c * g.incy, g.beta, g.ybin + c * g.incy * 2 * F);
     }
   }
   if (threadIdx.x == 0) g.tickets[blockIdx.x] = 0u;
 }
 
 template <int F>
-__global__ void __launch_bounds__(256) gemv_cols_kernel(GemvArgs g) {
-  if (g.vec) gemv_cols_body<F, 2>(g);
-  else gemv_cols_body<F, 1>(g);
+__global__ void __launch_bounds__(256, F <= 3 ? 3 : 2) gemv_cols_kernel(GemvArgs g) {
+  __shared__ double sm[(2 * F + 1) * 256];
+  if (g.vec) gemv_cols_body<F, 2>(g, sm);
+  else gemv_cols_body<F, 1>(g, sm);
 }
 
 // ---------------------------------------------------------------------------------------

@@ -92,7 +92,7 @@ struct GemvArgs {
   double* y;                  // kOutValue: values (stride incy)
   double* ybin;               // kOutBinned: binned states (stride incy states)
   long long incy;
-  int split;                  // rows kernel: warps per row (1, 2, 4, 8)
+  int split;                  // rows kernel: warps per row; cols kernel: row groups (1, 2, 4, 8)
   int vec;                    // 16-byte loads (alignment checked by the host)
   double* scratch;            // cols kernel: partial states
   unsigned* tickets;          // cols kernel: one per column block, zero on entry

@@ -138,6 +138,31 @@ def test_gemv_benchmark_shapes(cuda, rb, port, shape, ta):
     assert same_bits(Y.cpu().numpy(), want)
 
 
+# Column-reduction shapes (row-major, Trans: N outputs, M-long reductions). With 148 SMs they
+# select 1, 2, 4 and 8 row groups per CTA, each with 16-byte loads (N even) and scalar loads
+# (N odd).
+@pytest.mark.parametrize("shape", [(2, 2), (2, 3), (64, 8192), (64, 8191), (4096, 4096),
+                                   (3000, 600), (3000, 601), (20000, 3001), (5000, 130)])
+def test_gemv_column_reduction_shapes(cuda, rb, port, shape):
+    M, N = shape
+    rng = np.random.default_rng(7 * M + N)
+    A = np.exp2(rng.uniform(-25, 25, M * N)) * rng.choice([-1.0, 1.0], M * N)
+    x = rng.uniform(-1, 1, M)
+    y = rng.uniform(-1, 1, N)
+    want = y.copy()
+    port.rdgemv(3, b"r", b"t", M, N, 1.5, ptr(A), N, ptr(x), 1, 0.5, ptr(want), 1)
+    Y = dev(cuda, y)
+    rb.call("reproBLAS_rdgemv", 3, "r", "t", M, N, 1.5, dev(cuda, A), N, dev(cuda, x), 1, 0.5, Y, 1)
+    assert same_bits(Y.cpu().numpy(), want)
+    # binned form into existing states, fold 5
+    fold = 5
+    wantb = binned_zeros(fold, n=N)
+    port.dbdgemv(fold, b"r", b"t", M, N, 0.75, ptr(A), N, ptr(x), 1, ptr(wantb), 1)
+    Yb = dev(cuda, binned_zeros(fold, n=N))
+    rb.call("binnedBLAS_dbdgemv", fold, "r", "t", M, N, 0.75, dev(cuda, A), N, dev(cuda, x), 1, Yb, 1)
+    assert same_bits(Yb.cpu().numpy(), wantb)
+
+
 def test_gemm_2048_sampled(cuda, rb, port):
     """Plain binned dgemm, M=N=K=2048, uniform(-1,1), alpha 1.5, beta 0.5, fold 3: 512 sampled
     entries equal the oracle (each entry is binned(beta*C_ij) + binned dot of row and column);
