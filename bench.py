@@ -56,6 +56,8 @@ def parse():
     p.add_argument("--profile-kernel", choices=["int8", "plain_gemm", "gemv_n", "gemv_t"],
                    help="only run that kernel `--steps` times on an n^3 (or n^2) case, for ncu")
     p.add_argument("--profile-n", type=int, default=2048)
+    p.add_argument("--profile-m", type=int, default=0,
+                   help="rows of A for the gemv profile cases (default: --profile-n)")
     p.add_argument("--profile-slices", type=int, default=7)
     return p.parse_args()
 
@@ -540,28 +542,32 @@ def secondary(args):
         out["dgemm_int8_8192_s%d" % S] = rec
     del A, B, C
     out["batched"] = batched_case(torch, rb, rng)
-    # dgemv, NoTrans (row reduction) and Trans (column reduction), row-major A: 4096^2
-    # (134 MB, about L2's size: launch and host-call latency show) and 16384^2 (2.1 GB).
-    # "us" is CUDA-event time per call over back-to-back calls, "host_us" the host time of
-    # one call (the API call returns after enqueueing, so us ~ host_us means host-bound).
-    for m in (4096, 16384):
-        A = torch.from_numpy(rng.uniform(-1, 1, (m, m))).cuda()
-        x = torch.from_numpy(rng.uniform(-1, 1, m)).cuda()
-        y = torch.from_numpy(rng.uniform(-1, 1, m)).cuda()
+    # dgemv, NoTrans (row reduction) and Trans (column reduction), row-major A, alpha 1.5,
+    # beta 0.5, fold 3: the three 128 MiB shapes of the reference's gemv benchmark and
+    # 16384^2 (2 GiB). "us" is CUDA-event time per call over back-to-back calls, "host_us"
+    # the host time of one call (the call returns after enqueueing, so us ~ host_us would
+    # mean host-bound).
+    for (m, n) in ((4096, 4096), (16384, 1024), (1024, 16384), (16384, 16384)):
+        A = torch.from_numpy(rng.uniform(-1, 1, (m, n))).cuda()
         for ta in "nt":
-            call = lambda: rb.call("reproBLAS_rdgemv", 3, "r", ta, m, m, 1.5, A, m, x, 1, 0.5, y, 1)
-            reps = 20 if m == 4096 else 5
+            lx, ly = (n, m) if ta == "n" else (m, n)
+            x = torch.from_numpy(rng.uniform(-1, 1, lx)).cuda()
+            y = torch.from_numpy(rng.uniform(-1, 1, ly)).cuda()
+            call = lambda: rb.call("reproBLAS_rdgemv", 3, "r", ta, m, n, 1.5, A, n, x, 1, 0.5, y, 1)
+            reps = 5 if m * n > 2 ** 26 else 20
             t = _event_time(torch, call, reps, warm=3)
             torch.cuda.synchronize()
             h0 = time.perf_counter()
             call()
             h1 = time.perf_counter()
             torch.cuda.synchronize()
-            byts = 8.0 * m * m + 8 * 3 * m
-            out["dgemv_%d_%s" % (m, ta)] = {"gbs": round(byts / t / 1e9, 1), "us": round(t * 1e6, 2),
-                                            "host_us": round((h1 - h0) * 1e6, 1),
-                                            "frac_of_copy_peak": round(byts / t / 1e9 / peaks()[0], 3)}
-        del A, x, y
+            byts = 8.0 * m * n + 8.0 * lx + 16.0 * ly
+            out["dgemv_%dx%d_%s" % (m, n, ta)] = {
+                "gbs": round(byts / t / 1e9, 1), "us": round(t * 1e6, 2),
+                "host_us": round((h1 - h0) * 1e6, 1),
+                "frac_of_copy_peak": round(byts / t / 1e9 / peaks()[0], 3)}
+            del x, y
+        del A
     return out
 
 
@@ -571,19 +577,26 @@ def profile_case(args):
     import reproblas_b200 as rb
     rng = np.random.default_rng(1)
     n = args.profile_n
+    if args.profile_kernel in ("gemv_n", "gemv_t"):
+        m = args.profile_m or n
+        ta = args.profile_kernel[-1]
+        A = torch.from_numpy(rng.uniform(-1, 1, (m, n))).cuda()
+        x = torch.from_numpy(rng.uniform(-1, 1, n if ta == "n" else m)).cuda()
+        y = torch.from_numpy(rng.uniform(-1, 1, m if ta == "n" else n)).cuda()
+        for _ in range(args.warmup + args.steps):
+            rb.call("reproBLAS_rdgemv", 3, "r", ta, m, n, 1.5, A, n, x, 1, 0.5, y, 1)
+        torch.cuda.synchronize()
+        print("profile case done: %s m=%d n=%d" % (args.profile_kernel, m, n))
+        return
     A = torch.from_numpy(int8_operands(rng, n, n)).cuda()
     B = torch.from_numpy(int8_operands(rng, n, n)).cuda()
     C = torch.from_numpy(rng.uniform(-1, 1, (n, n))).cuda()
-    x = torch.from_numpy(rng.uniform(-1, 1, n)).cuda()
-    y = torch.from_numpy(rng.uniform(-1, 1, n)).cuda()
     for _ in range(args.warmup + args.steps):
         if args.profile_kernel == "int8":
             rb.call("rb_dgemm_int8", 3, "r", "n", "n", n, n, n, 1.5, A, n, B, n, 0.5, C, n,
                     args.profile_slices)
-        elif args.profile_kernel == "plain_gemm":
-            rb.call("reproBLAS_rdgemm", 3, "r", "n", "n", n, n, n, 1.5, A, n, B, n, 0.5, C, n)
         else:
-            rb.call("reproBLAS_rdgemv", 3, "r", args.profile_kernel[-1], n, n, 1.5, A, n, x, 1, 0.5, y, 1)
+            rb.call("reproBLAS_rdgemm", 3, "r", "n", "n", n, n, n, 1.5, A, n, B, n, 0.5, C, n)
     torch.cuda.synchronize()
     print("profile case done: %s n=%d" % (args.profile_kernel, n))
 

@@ -5,6 +5,9 @@
 // (src/binnedBLAS/dbdgemv.ccog:146-158); dgemm uses general operand strides. Host operands
 // are copied to a device workspace first; outputs are copied back before returning.
 #include <cstring>
+#include <map>
+#include <string>
+#include <utility>
 
 #include "rb_host.h"
 #include "../../include/reproblas_b200.h"
@@ -69,6 +72,160 @@ struct GemvReq {
   int mode;
 };
 
+// fl(alpha * x_i) into a contiguous buffer zero-padded to npad entries, for the TMA-fed
+// kernels when x is strided or misaligned; the product is the one dbdgemv forms before its
+// dots.
+__global__ void scale_x_kernel(const double* x, long long n, long long incx, double alpha,
+                               double* bx, long long npad) {
+  const long long step = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < npad; i += step) {
+    double v = 0.0;
+    if (i < n) {
+      v = x[i * incx];
+      if (alpha != 1.0) v = __dmul_rn(v, alpha);
+    }
+    bx[i] = v;
+  }
+}
+
+// CTAs per SM of the TMA-fed kernels, per (device, fold); the first query also opts the
+// kernels in to their shared memory on that device. Returns -1 on a CUDA error (recorded),
+// 0 when a kernel does not fit on an SM, 1 otherwise.
+int stream_occupancy(const Blas23FoldOps* o, int device, int fold, int* rows_per_sm,
+                      int* cols_per_sm) {
+  static std::mutex mu;
+  static std::map<std::pair<int, int>, std::pair<int, int>> cache;
+  std::lock_guard<std::mutex> g(mu);
+  auto key = std::make_pair(device, fold);
+  auto it = cache.find(key);
+  if (it == cache.end()) {
+    int r = 0, c = 0;
+    if (!cuda_ok(o->gemv_stream_prepare(&r, &c), "gemv stream kernel attributes")) return -1;
+    it = cache.emplace(key, std::make_pair(r, c)).first;
+  }
+  *rows_per_sm = it->second.first;
+  *cols_per_sm = it->second.second;
+  return (*rows_per_sm > 0 && *cols_per_sm > 0) ? 1 : 0;
+}
+
+// dgemv through the TMA-fed kernels (rb_gemv_stream.cuh). The caller checked: alpha != 0,
+// lda even, A 16-byte aligned (or on the host), dimensions below 2^31.
+bool run_gemv_stream(const GemvReq& q, const Blas23FoldOps* o, Workspace* w, const DeviceInfo& di,
+                     bool nt, long long Rs, long long Cs, int rows_per_sm, int cols_per_sm) {
+  cudaStream_t s = w->stream;
+  const long long nout = nt ? Rs : Cs, nred = nt ? Cs : Rs;
+  const long long REC = 2 * q.fold + 1;
+  GemvStreamArgs g{};
+  g.R = Rs;
+  g.C = Cs;
+  // G thread groups per output (2, 4 or 8): units are bands of P = 512/G rows (stages of
+  // 16G columns) or blocks of P columns (stages of 8G rows), split evenly over one CTA per
+  // resident slot (every CTA gets at least one stage). Take the smallest G for which the
+  // last CTA of a cut unit merges at most about 4 parts per thread.
+  const long long gmax = (long long)di.sms * (nt ? rows_per_sm : cols_per_sm);
+  int G = 2;
+  long long nunits = 0, nb = 0, T = 0, grid = 0;
+  for (;;) {
+    const long long P = 512 / G;
+    nunits = (nout + P - 1) / P;
+    nb = nt ? (nred + 16 * G - 1) / (16 * G) : (nred + 8 * G - 1) / (8 * G);
+    T = nunits * nb;
+    grid = T < gmax ? T : gmax;
+    // a unit meets at most ceil((nb-1) / min_range) + 1 CTA ranges, min_range = floor(T/grid)
+    const long long parts = nb / (T / grid) + 2;
+    if ((parts + G - 1) / G <= 4 || G == 8) break;
+    G *= 2;
+  }
+  g.groups = G;
+  g.kslots = nb / (T / grid) + 2;
+  const long long ntickets = nunits;
+  const size_t part_bytes = (size_t)nout * g.kslots * REC * 8;
+  if (!w->ensure_tickets((size_t)ntickets)) return false;
+
+  const size_t per_out = q.mode == kOutValue ? 8 : (size_t)2 * q.fold * 8;
+  const size_t a_bytes = ((size_t)(Rs - 1) * q.lda + Cs) * 8;
+  const size_t x_bytes = span(nred, q.incX, 8);
+  const size_t y_bytes = q.mode == kOutValue ? span(nout, q.incY, 8)
+                                             : ((size_t)(nout - 1) * q.incY + 1) * per_out;
+  const bool a_host = !on_device(q.A), x_host = !on_device(q.X), y_host = !on_device(q.Y);
+  // x is read in place when unit-stride and 16-byte aligned (host copies are aligned);
+  // otherwise fl(alpha*x) is gathered into bx by a small kernel first
+  const bool x_direct = q.incX == 1 && (x_host || ((uintptr_t)q.X % 16) == 0);
+  const size_t need = part_bytes + (x_direct ? 0 : (size_t)nred * 8) + (a_host ? a_bytes : 0) +
+                      (x_host ? x_bytes : 0) + (y_host ? y_bytes : 0) + 6 * 256;
+  if (!w->ensure_big(need)) return false;
+  Bump b{w->big};
+  bool ok = true;
+  const double* dA = (const double*)to_device(q.A, a_bytes, &b, s, &ok);
+  const double* dX = (const double*)to_device(q.X, x_bytes, &b, s, &ok);
+  double* dY = (double*)to_device(q.Y, y_bytes, &b, s, &ok);
+  double* bx = x_direct ? nullptr : (double*)b.take((size_t)nred * 8);
+  double* part = (double*)b.take(part_bytes);
+  if (!ok) return false;
+
+  auto enc = tensor_map_encoder();
+  if (!enc) {
+    set_error(RB_ERR_CUDA, "gemv: cuTensorMapEncodeTiled is unavailable");
+    return false;
+  }
+  CUtensorMap tm, tmx;
+  cuuint64_t dims[2] = {(cuuint64_t)Cs, (cuuint64_t)Rs};
+  cuuint64_t strides[1] = {(cuuint64_t)q.lda * 8};
+  // rows kernel: boxes of 16 columns x P rows, 128-byte swizzle; cols kernel: P x 8G
+  const cuuint32_t P = 512u / (cuuint32_t)G;
+  cuuint32_t box[2] = {nt ? 16u : P, nt ? P : 8u * (cuuint32_t)G};
+  cuuint32_t estr[2] = {1u, 1u};
+  CUresult r = enc(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void*)dA, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   nt ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  // x (or bx): boxes of one stage's 16G (rows kernel) or 8G (cols kernel) entries (a rank-1
+  // map reads no stride)
+  cuuint64_t xdims[1] = {(cuuint64_t)nred};
+  cuuint32_t xbox[1] = {nt ? 16u * (cuuint32_t)G : 8u * (cuuint32_t)G};
+  if (r == CUDA_SUCCESS)
+    r = enc(&tmx, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 1, (void*)(x_direct ? dX : bx), xdims, strides,
+            xbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error(RB_ERR_CUDA, "gemv: cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return false;
+  }
+
+  g.alpha = q.alpha;
+  g.scale_x = x_direct && q.alpha != 1.0;
+  g.beta = q.beta;
+  g.mode = q.mode;
+  g.y = q.mode == kOutValue ? dY : nullptr;
+  g.ybin = q.mode == kOutBinned ? dY : nullptr;
+  g.incy = q.incY;
+  g.scratch = part;
+  g.tickets = w->tickets;
+  g.status = w->dstatus();
+  if (!x_direct) {
+    count_launch();
+    long long sgrid = (nred + 255) / 256;
+    if (sgrid > (long long)di.sms * 4) sgrid = (long long)di.sms * 4;
+    scale_x_kernel<<<(unsigned)sgrid, 256, 0, s>>>(dX, nred, q.incX, q.alpha, bx, nred);
+    if (!cuda_ok(cudaGetLastError(), "gemv scale launch")) return false;
+  }
+  count_launch();
+  if (!cuda_ok(o->gemv_stream(g, tm, tmx, nt, (int)grid, s), "gemv launch")) return false;
+  if (y_host) {
+    int* hs = w->hstatus();
+    if (!cuda_ok(cudaMemcpyAsync(q.Y, dY, y_bytes, cudaMemcpyDeviceToHost, s), "copy y") ||
+        !cuda_ok(cudaMemcpyAsync(hs, w->dstatus(), 4, cudaMemcpyDeviceToHost, s), "copy status") ||
+        !cuda_ok(cudaStreamSynchronize(s), "cudaStreamSynchronize"))
+      return false;
+    if (*hs != 0) {
+      cudaMemsetAsync(w->dstatus(), 0, 4, s);
+      set_error(RB_ERR_CUDA, "gemv: a pipeline wait timed out (affected entries are NaN)");
+      return false;
+    }
+  }
+  return true;
+}
+
 bool run_gemv(const GemvReq& q) {
   if (q.M == 0 || q.N == 0) return true;   // rdgemv.c:43-45
   const Blas23FoldOps* o = ops23(q.fold);
@@ -104,6 +261,17 @@ bool run_gemv(const GemvReq& q) {
   // 16-byte loads when rows (and x for the row kernel) are 16-byte aligned
   const bool a_al = (q.lda % 2) == 0;
   const bool vec = nt ? (a_al && q.incX == 1) : (a_al && (nout % 2) == 0);
+  // TMA-fed kernels: row pitch a multiple of 16 bytes, A 16-byte aligned (host operands are
+  // copied to aligned device memory), tensor coordinates within int, and rows long enough /
+  // outputs numerous enough to fill the ring's boxes
+  const bool a_ptr_al = !on_device(q.A) || ((uintptr_t)q.A % 16) == 0;
+  if (o->gemv_stream && nred_eff > 0 && a_al && a_ptr_al && Rs < (1ll << 31) && Cs < (1ll << 31) &&
+      (nt ? nred_eff >= 512 : nout >= 128)) {
+    int rps = 0, cps = 0;
+    const int occ = stream_occupancy(o, di.device, q.fold, &rps, &cps);
+    if (occ < 0) return false;
+    if (occ > 0) return run_gemv_stream(q, o, w, di, nt, Rs, Cs, rps, cps);
+  }
   int groups = 1;
   if (!nt) {
     // Column kernel shape: G row groups per CTA, T = 256/G threads per group, W columns per

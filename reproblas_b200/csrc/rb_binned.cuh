@@ -358,6 +358,46 @@ template <typename T, int F> struct Acc {
   }
 };
 
+// Deposit K values into each of two accumulators (all K counted as elements; zeros deposit
+// nothing). Same result as a.tile<K>(va, K); b.tile<K>(vb, K), but in the common case (finite
+// values, neither accumulator at index 0) the two deposit chains sit in one straight-line
+// block, so their latencies overlap.
+template <typename T, int F, int K>
+__device__ __forceinline__ void tile2(Acc<T, F>& a, const T (&va)[K], Acc<T, F>& b,
+                                      const T (&vb)[K]) {
+  using B = BT<T>;
+  unsigned ma = 0, mb = 0;
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    const unsigned ka = B::key(va[k]), kb = B::key(vb[k]);
+    ma = ka > ma ? ka : ma;
+    mb = kb > mb ? kb : mb;
+  }
+  if (ma >= B::kInfKey || mb >= B::kInfKey) {
+    a.template tile<K>(va, K);
+    b.template tile<K>(vb, K);
+    return;
+  }
+  a.prepare(ma, K);
+  b.prepare(mb, K);
+  if (a.idx != 0 && b.idx != 0) {
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      a.deposit(va[k]);
+      b.deposit(vb[k]);
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      if (a.idx == 0) a.deposit0(va[k]); else a.deposit(va[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      if (b.idx == 0) b.deposit0(vb[k]); else b.deposit(vb[k]);
+    }
+  }
+}
+
 // binned_ddmconv (src/binned/ddmconv.c:23-81): fixed-order conversion to double with
 // scaling when the index is within 3 of the top.
 template <int F>

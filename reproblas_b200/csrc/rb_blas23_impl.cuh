@@ -13,6 +13,7 @@
 #pragma once
 #include "rb_binned.cuh"
 #include "rb_kernels.cuh"
+#include "rb_ptx.cuh"
 
 namespace rb {
 
@@ -28,13 +29,15 @@ __device__ __forceinline__ void init_from_value(Acc<double, F>& a, double y, dou
 }
 
 // Epilogue shared by the BLAS2/3 kernels: combine the products' state `a` (renormalised)
-// with the entry's initial state and write the result.
+// with the entry's initial state and write the result. `yv` is *out_value, loaded by the
+// caller (kOutValue only), so that the load can be issued early.
 template <int F>
-__device__ __forceinline__ void finish_entry(Acc<double, F>& a, int mode, double* out_value,
-                                             double beta, double* out_binned) {
+__device__ __forceinline__ void finish_entry_pre(Acc<double, F>& a, int mode, double yv,
+                                                 double* out_value, double beta,
+                                                 double* out_binned) {
   if (mode == kOutValue) {
     Acc<double, F> init;
-    init_from_value(init, *out_value, beta);
+    init_from_value(init, yv, beta);
     init.merge(a);
     init.renorm();
     double p[F], c[F];
@@ -47,6 +50,12 @@ __device__ __forceinline__ void finish_entry(Acc<double, F>& a, int mode, double
     prev.renorm();
     prev.store(out_binned, out_binned + F, 1);
   }
+}
+
+template <int F>
+__device__ __forceinline__ void finish_entry(Acc<double, F>& a, int mode, double* out_value,
+                                             double beta, double* out_binned) {
+  finish_entry_pre<F>(a, mode, mode == kOutValue ? *out_value : 0.0, out_value, beta, out_binned);
 }
 
 __device__ __forceinline__ void ld2(const double* p, double& a, double& b) {
@@ -459,11 +468,25 @@ cudaError_t launch_gemm(const GemmArgs& g, cudaStream_t s, int* bm, int* bn) {
   return cudaGetLastError();
 }
 
+}  // namespace rb
+
+#include "rb_gemv_stream.cuh"
+
+namespace rb {
+
 template <int F>
 Blas23FoldOps make_blas23_ops() {
   Blas23FoldOps o;
   o.gemv = launch_gemv<F>;
   o.gemm = launch_gemm<F>;
+  // the TMA-fed gemv kernels fit their registers (17 warps per SM) up to fold 3
+  if constexpr (F <= 3) {
+    o.gemv_stream = gs::launch_gemv_stream<F>;
+    o.gemv_stream_prepare = gs::prepare_gemv_stream<F>;
+  } else {
+    o.gemv_stream = nullptr;
+    o.gemv_stream_prepare = nullptr;
+  }
   return o;
 }
 

@@ -3,6 +3,7 @@
 // launch-shape selection.
 #pragma once
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <atomic>
 #include <cstdint>
@@ -26,6 +27,10 @@ LaunchShape launch_shape();   // user override or defaults (0 = default)
 
 struct DeviceInfo { int device; int sms; };
 bool device_info(DeviceInfo* out);
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link), or
+// nullptr when the driver does not provide it.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 
 // ---- pointers ---------------------------------------------------------------------------
 enum class Mem { Device, Pinned, Pageable };
@@ -63,6 +68,8 @@ struct Workspace {
   size_t ntickets = 0;
 
   double* dacc() { return (double*)dsmall; }                  // 1024 B accumulator slot
+  int* dstatus() { return (int*)(dsmall + 2048); }             // kernel status word (0 = ok)
+  int* hstatus() { return (int*)(hsmall + 2048); }
   double* dscale() { return (double*)(dsmall + 1024); }        // 8 B
   void* dresult() { return (void*)(dsmall + 1088); }           // 64 B result slot
   double* hacc() { return (double*)hsmall; }

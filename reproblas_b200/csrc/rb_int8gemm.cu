@@ -13,25 +13,11 @@ namespace {
 
 long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
 
-// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link).
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-  });
-  return fn;
-}
-
 // 4-D map of a slice array in the pre-tiled layout [Kp/16][S][rows/8][128 B], with a box of
 // 128 B x box_rows/8 row groups x S slices x 2 K columns (one pipeline stage).
 bool encode_slices(CUtensorMap* m, const int8_t* base, long long Kp, long long rows, int S,
                    int box_rows) {
-  auto fn = encode_fn();
+  auto fn = tensor_map_encoder();
   if (!fn) {
     set_error(RB_ERR_CUDA, "rb_dgemm_int8: cuTensorMapEncodeTiled is unavailable");
     return false;

@@ -27,6 +27,7 @@
 
 #include "rb_binned.cuh"
 #include "rb_kernels.cuh"
+#include "rb_ptx.cuh"
 
 namespace rb {
 namespace i8 {
@@ -46,47 +47,7 @@ __host__ __device__ constexpr long long max_k_chunk(int S) {
   return (2147483647ll / ((long long)S * 127 * 127)) / BK * BK;
 }
 
-// ---- small PTX helpers ------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-
-__device__ __forceinline__ void fence_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t addr, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(addr), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint32_t addr, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(addr), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait: gives up after ~2 s and reports false.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t addr, unsigned parity) {
-  for (long long it = 0; it < (1ll << 25); it++) {
-    if (mbar_try_wait(addr, parity)) return true;
-    if (it > 1024) __nanosleep(64);
-  }
-  return false;
-}
-
+// ---- tcgen05 helpers (the generic mbarrier / bulk-copy helpers are in rb_ptx.cuh) -------
 __device__ __forceinline__ void tc_fence_before() {
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 }
@@ -153,15 +114,6 @@ __device__ __forceinline__ void tma_load_4d(uint32_t dst, const void* tmap, int 
       :
       : "r"(dst), "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(mbar)
       : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes)
-               : "memory");
-}
-
-__device__ __forceinline__ void fence_barrier_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }

@@ -1,6 +1,7 @@
 // rb_kernels.cuh -- launch-parameter structs and kernel entry points shared between the
 // CUDA translation units and the host-side C ABI (rb_api.cu).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -111,9 +112,31 @@ struct GemmArgs {
   long long sci, scj;         // C_ij at offset i*sci + j*scj (values or states)
 };
 
+// TMA-fed dgemv (rb_gemv_stream.cuh): A is R x C row-major behind a 2-D tensor map.
+struct GemvStreamArgs {
+  long long R, C;        // A is R x C (row-major view)
+  double alpha;          // multiplies the x the kernel reads when scale_x is set
+  int scale_x;           // 0: the x tensor holds fl(alpha*x) already
+  double beta;
+  int mode;              // kOutValue / kOutBinned
+  double* y;             // kOutValue: values (stride incy)
+  double* ybin;          // kOutBinned: binned states (stride incy states)
+  long long incy;
+  double* scratch;       // partial states
+  unsigned* tickets;     // one per band (rows) / column block (cols), zero on entry
+  int* status;           // set to 2 when a pipeline wait gives up
+  long long kslots;      // partial-state slots per output of a unit cut between CTAs
+  int groups;            // thread groups per output (power of two, 1..8)
+};
+
 struct Blas23FoldOps {
   cudaError_t (*gemv)(const GemvArgs& g, bool rows, dim3 grid, cudaStream_t s);
   cudaError_t (*gemm)(const GemmArgs& g, cudaStream_t s, int* bm, int* bn);
+  // TMA-fed dgemv (nullptr for folds it does not cover)
+  cudaError_t (*gemv_stream)(const GemvStreamArgs& g, const CUtensorMap& tm, const CUtensorMap& tmx,
+                             bool rows, int grid, cudaStream_t s);
+  // opt in to the stream kernels' shared memory; CTAs per SM of each
+  cudaError_t (*gemv_stream_prepare)(int* rows_per_sm, int* cols_per_sm);
 };
 extern const Blas23FoldOps blas23_fold2, blas23_fold3, blas23_fold4, blas23_fold5,
     blas23_fold6, blas23_fold7, blas23_fold8;

@@ -119,6 +119,19 @@ bool Workspace::ensure_tickets(size_t n) {
   return true;
 }
 
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  });
+  return fn;
+}
+
 static bool init_workspace(Workspace* w, int dev, cudaStream_t s, int sms) {
   w->device = dev;
   w->stream = s;
@@ -131,7 +144,9 @@ static bool init_workspace(Workspace* w, int dev, cudaStream_t s, int sms) {
     set_error(RB_ERR_ALLOC, "workspace allocation failed");
     return false;
   }
-  if (!cuda_ok(cudaMemset(w->scratch.ticket, 0, 256), "cudaMemset")) return false;
+  if (!cuda_ok(cudaMemset(w->scratch.ticket, 0, 256), "cudaMemset") ||
+      !cuda_ok(cudaMemset(w->dsmall, 0, Workspace::kSmallBytes), "cudaMemset"))
+    return false;
   if (!cuda_ok(cudaMallocHost(&w->hsmall, Workspace::kSmallBytes), "cudaMallocHost")) return false;
   if (!cuda_ok(cudaStreamCreateWithFlags(&w->copy_stream, cudaStreamNonBlocking),
                "cudaStreamCreate"))

@@ -138,9 +138,9 @@ def test_gemv_benchmark_shapes(cuda, rb, port, shape, ta):
     assert same_bits(Y.cpu().numpy(), want)
 
 
-# Column-reduction shapes (row-major, Trans: N outputs, M-long reductions). With 148 SMs they
-# select 1, 2, 4 and 8 row groups per CTA, each with 16-byte loads (N even) and scalar loads
-# (N odd).
+# Column-reduction shapes (row-major, Trans: N outputs, M-long reductions). Even N takes the
+# TMA-fed kernel, whose thread groups per output (2, 4, 8) these shapes vary, odd N (odd lda)
+# the register-streaming kernel with its row groups (1, 2, 4, 8).
 @pytest.mark.parametrize("shape", [(2, 2), (2, 3), (64, 8192), (64, 8191), (4096, 4096),
                                    (3000, 600), (3000, 601), (20000, 3001), (5000, 130)])
 def test_gemv_column_reduction_shapes(cuda, rb, port, shape):
@@ -188,3 +188,27 @@ def test_gemm_2048_sampled(cuda, rb, port):
     rb.call("reproBLAS_rdgemm", 3, "c", "t", "t", n, n, n, 1.5, dev(cuda, A), n, dev(cuda, B), n,
             0.5, Ct, n)
     assert same_bits(Ct.cpu().numpy().reshape(n, n).T, got)
+
+
+@pytest.mark.parametrize("ta", ["n", "t"])
+def test_gemv_x_layouts(cuda, rb, port, ta):
+    """x read in place (unit stride, aligned), through a gathered copy (stride 3, or unit
+    stride at an odd 8-byte offset), alpha 1 and not, fold 2 and 3."""
+    M, N = 1000, 1200
+    rng = np.random.default_rng(11)
+    A = rng.uniform(-1, 1, M * N)
+    lx, ly = (N, M) if ta == "n" else (M, N)
+    buf = rng.uniform(-1, 1, 3 * lx + 1)
+    y0 = rng.uniform(-1, 1, ly)
+    dA = dev(cuda, A)
+    dbuf = dev(cuda, buf)
+    for fold in (2, 3):
+        for alpha in (1.0, 1.5):
+            for off, inc in ((0, 1), (1, 1), (0, 3)):
+                xs = buf[off:off + (lx - 1) * inc + 1]
+                want = y0.copy()
+                port.rdgemv(fold, b"r", ta.encode(), M, N, alpha, ptr(A), N, ptr(xs), inc, 0.5,
+                            ptr(want), 1)
+                Y = dev(cuda, y0)
+                rb.call("reproBLAS_rdgemv", fold, "r", ta, M, N, alpha, dA, N, dbuf[off:], inc, 0.5, Y, 1)
+                assert same_bits(Y.cpu().numpy(), want), (fold, alpha, off, inc)
