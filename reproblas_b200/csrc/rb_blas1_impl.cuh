@@ -238,8 +238,11 @@ template <typename T> struct VecW;
 template <> struct VecW<double> { static constexpr int n = 2; };
 template <> struct VecW<float> { static constexpr int n = 4; };
 
+// The scaled sum of squares carries a scale next to its accumulator; it is held to four CTAs
+// per SM (64 registers), which pays for a few spills. (A minimum of 0 leaves the others to
+// the compiler's own choice.)
 template <typename T, int F, int OP, bool VEC>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, OP == kOpSsq ? 4 : 0)
 blas1_kernel(Blas1Args args) {
   constexpr int VW = VecW<T>::n;     // elements per 16-byte vector
   constexpr int NV = 4;              // vectors per thread per warp tile
@@ -413,8 +416,9 @@ template <> struct Pair<float> {
   static __device__ __forceinline__ V ld(const float* p) { return __ldg((const float2*)p); }
 };
 
+// Three CTAs per SM for double complex (80 registers), four for float complex.
 template <typename T, int F, int OP>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 3 : 4)
 blasc_kernel(Blas1Args args) {
   constexpr int REC = 4 * F + 2;
   constexpr int K = OP == kOpCSum ? 8 : 4;   // complex elements per thread per step
@@ -444,8 +448,9 @@ blasc_kernel(Blas1Args args) {
           nv = k + 1;
         }
       }
-      st.re.template tile<K>(vr, nv);
-      st.im.template tile<K>(vi, nv);
+      // zeros past the end deposit nothing; counting them only renormalises earlier
+      if (nv == K) tile2<T, F, K>(st.re, vr, st.im, vi);
+      else { st.re.template tile<K>(vr, nv); st.im.template tile<K>(vi, nv); }
     } else {
       // conj(x)*y: real part receives xr*yr and xi*yi, imaginary part xr*yi and
       // -(xi*yr), each product deposited separately (depositDotC.py:14-23)
@@ -465,8 +470,8 @@ blasc_kernel(Blas1Args args) {
           nv = 2 * k + 2;
         }
       }
-      st.re.template tile<2 * K>(vr, nv);
-      st.im.template tile<2 * K>(vi, nv);
+      if (nv == 2 * K) tile2<T, F, 2 * K>(st.re, vr, st.im, vi);
+      else { st.re.template tile<2 * K>(vr, nv); st.im.template tile<2 * K>(vi, nv); }
     }
   }
 
