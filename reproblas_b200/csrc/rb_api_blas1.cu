@@ -49,8 +49,8 @@ cudaError_t launch(const Blas1Req& r, bool vec, int grid, int block, const Blas1
   switch (r.type) {
     case 'd': return launch_blas1_d(r.fold, r.op, vec, grid, block, a, s);
     case 's': return launch_blas1_s(r.fold, r.op, vec, grid, block, a, s);
-    case 'z': return launch_blas1_z(r.fold, r.op, grid, block, a, s);
-    default: return launch_blas1_c(r.fold, r.op, grid, block, a, s);
+    case 'z': return launch_blas1_z(r.fold, r.op, vec, grid, block, a, s);
+    default: return launch_blas1_c(r.fold, r.op, vec, grid, block, a, s);
   }
 }
 
@@ -60,14 +60,16 @@ void plan_vector(const Blas1Req& r, const void* x, long long incx, const void* y
   *vec = false;
   *head = n;
   *body_end = n;
-  if (comps(r.type) != 1 || incx != 1 || (is_dot(r) && incy != 1)) return;
-  const size_t eb = elem_bytes(r.type);
+  if (incx != 1 || (is_dot(r) && incy != 1)) return;
+  const size_t eb = elem_bytes(r.type);   // bytes per (complex) element
   uintptr_t ax = (uintptr_t)x, ay = (uintptr_t)y;
   if (ax % eb != 0 || (is_dot(r) && ay % eb != 0)) return;
   long long h = (long long)(((16 - ax % 16) % 16) / eb);
   if (is_dot(r) && ((ay + h * eb) % 16) != 0) return;
   if (h > n) h = n;
-  const long long wt = 32 * 4 * (long long)(16 / eb);   // elements per warp tile
+  // elements per warp tile
+  const long long wt = comps(r.type) == 1 ? 32 * 4 * (long long)(16 / eb)
+                                          : blas1_complex_tile(eb, r.op);
   *vec = true;
   *head = h;
   *body_end = h + ((n - h) / wt) * wt;

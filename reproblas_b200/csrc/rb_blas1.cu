@@ -34,15 +34,15 @@ cudaError_t launch_blas1_s(int fold, int op, bool vec, int grid, int block, cons
   const Blas1FoldOps* o = fold_ops(fold);
   return o ? o->real_s(op, vec, grid, block, a, s) : cudaErrorInvalidValue;
 }
-cudaError_t launch_blas1_z(int fold, int op, int grid, int block, const Blas1Args& a,
+cudaError_t launch_blas1_z(int fold, int op, bool vec, int grid, int block, const Blas1Args& a,
                            cudaStream_t s) {
   const Blas1FoldOps* o = fold_ops(fold);
-  return o ? o->cplx_z(op, grid, block, a, s) : cudaErrorInvalidValue;
+  return o ? o->cplx_z(op, vec, grid, block, a, s) : cudaErrorInvalidValue;
 }
-cudaError_t launch_blas1_c(int fold, int op, int grid, int block, const Blas1Args& a,
+cudaError_t launch_blas1_c(int fold, int op, bool vec, int grid, int block, const Blas1Args& a,
                            cudaStream_t s) {
   const Blas1FoldOps* o = fold_ops(fold);
-  return o ? o->cplx_c(op, grid, block, a, s) : cudaErrorInvalidValue;
+  return o ? o->cplx_c(op, vec, grid, block, a, s) : cudaErrorInvalidValue;
 }
 cudaError_t launch_merge_states(int fold, int count, const double* states, double* out,
                                 cudaStream_t s) {

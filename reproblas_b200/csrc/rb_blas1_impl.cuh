@@ -417,11 +417,19 @@ template <> struct Pair<float> {
 };
 
 // Three CTAs per SM for double complex (80 registers), four for float complex.
-template <typename T, int F, int OP>
+// VEC: the body [head, body_end) is read in warp tiles of 16-byte vectors (contiguous,
+// aligned inputs; the host plans head and body_end with blas1_complex_tile()); everything
+// else, or all of a strided input, goes through the element path.
+template <typename T, int F, int OP, bool VEC>
 __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 3 : 4)
 blasc_kernel(Blas1Args args) {
   constexpr int REC = 4 * F + 2;
-  constexpr int K = OP == kOpCSum ? 8 : 4;   // complex elements per thread per step
+  constexpr int K = OP == kOpCSum ? 8 : 4;   // element path: complex elements per step
+  constexpr int VW = 16 / (2 * sizeof(T));   // complex elements per 16-byte vector
+  constexpr int NV = OP == kOpCSum ? 4 : 2;  // vectors per lane per warp tile
+  constexpr int E = NV * VW;                 // complex elements per lane per warp tile
+  constexpr int WT = 32 * E;
+  static_assert(WT == blas1_complex_tile(sizeof(T) * 2, OP), "tile mismatch with the host");
   __shared__ T smem[32 * REC];
   using B = BT<T>;
 
@@ -429,21 +437,65 @@ blasc_kernel(Blas1Args args) {
   const T* __restrict__ y = (const T*)args.y;
   const long long nthreads = (long long)gridDim.x * blockDim.x;
   const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
 
   RedC<T, F, OP> st;
   st.init();
 
+  long long head = args.n, body_end = args.n;
+  if (VEC) {
+    head = args.head;
+    body_end = args.body_end;
+    const long long nwt = (body_end - head) / WT;
+    const long long gwarp = gtid >> 5, nwarps = nthreads >> 5;
 #pragma unroll 1
-  for (long long b = gtid; b < args.n; b += K * nthreads) {
+    for (long long wt = gwarp; wt < nwt; wt += nwarps) {
+      const long long base = head + wt * WT;   // complex element index
+      T xr[E], xi[E];
+#pragma unroll
+      for (int k = 0; k < NV; k++) {
+        T t[2 * VW];
+        ldv(x + 2 * (base + (long long)(k * 32 + lane) * VW), t);
+#pragma unroll
+        for (int j = 0; j < VW; j++) { xr[k * VW + j] = t[2 * j]; xi[k * VW + j] = t[2 * j + 1]; }
+      }
+      if constexpr (OP == kOpCSum) {
+        tile2<T, F, E>(st.re, xr, st.im, xi);
+      } else {
+        T vr[2 * E], vi[2 * E];
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+          T t[2 * VW];
+          ldv(y + 2 * (base + (long long)(k * 32 + lane) * VW), t);
+#pragma unroll
+          for (int j = 0; j < VW; j++) {
+            const int e = k * VW + j;
+            vr[2 * e] = B::mul(xr[e], t[2 * j]);
+            vr[2 * e + 1] = B::mul(xi[e], t[2 * j + 1]);
+            vi[2 * e] = B::mul(xr[e], t[2 * j + 1]);
+            vi[2 * e + 1] = -B::mul(xi[e], t[2 * j]);
+          }
+        }
+        tile2<T, F, 2 * E>(st.re, vr, st.im, vi);
+      }
+    }
+  }
+
+  // Element path: the head and tail around the vector body, or everything when the input
+  // is strided or not aligned.
+  const long long S = head + (args.n - body_end);
+#pragma unroll 1
+  for (long long b = gtid; b < S; b += K * nthreads) {
     if (OP == kOpCSum) {
       T vr[K], vi[K];
       int nv = 0;
 #pragma unroll
       for (int k = 0; k < K; k++) {
-        long long i = b + k * nthreads;
+        const long long i = b + k * nthreads;
         vr[k] = T(0); vi[k] = T(0);
-        if (i < args.n) {
-          auto v = Pair<T>::ld(x + 2 * i * args.incx);
+        if (i < S) {
+          const long long e = i < head ? i : body_end + (i - head);
+          auto v = Pair<T>::ld(x + 2 * e * args.incx);
           vr[k] = v.x; vi[k] = v.y;
           nv = k + 1;
         }
@@ -458,11 +510,12 @@ blasc_kernel(Blas1Args args) {
       int nv = 0;
 #pragma unroll
       for (int k = 0; k < K; k++) {
-        long long i = b + k * nthreads;
+        const long long i = b + k * nthreads;
         vr[2 * k] = vr[2 * k + 1] = vi[2 * k] = vi[2 * k + 1] = T(0);
-        if (i < args.n) {
-          auto xv = Pair<T>::ld(x + 2 * i * args.incx);
-          auto yv = Pair<T>::ld(y + 2 * i * args.incy);
+        if (i < S) {
+          const long long e = i < head ? i : body_end + (i - head);
+          auto xv = Pair<T>::ld(x + 2 * e * args.incx);
+          auto yv = Pair<T>::ld(y + 2 * e * args.incy);
           vr[2 * k] = B::mul(xv.x, yv.x);
           vr[2 * k + 1] = B::mul(xv.y, yv.y);
           vi[2 * k] = B::mul(xv.x, yv.y);
@@ -576,10 +629,16 @@ cudaError_t launch_real(int op, bool vec, int grid, int block, const Blas1Args& 
 }
 
 template <typename T, int F>
-cudaError_t launch_cplx(int op, int grid, int block, const Blas1Args& a, cudaStream_t s) {
-  if (op == kOpCSum) blasc_kernel<T, F, kOpCSum><<<grid, block, 0, s>>>(a);
-  else if (op == kOpCDotc && sizeof(T) == 8) blasc_kernel<T, F, kOpCDotc><<<grid, block, 0, s>>>(a);
-  else return cudaErrorInvalidValue;
+cudaError_t launch_cplx(int op, bool vec, int grid, int block, const Blas1Args& a, cudaStream_t s) {
+  if (op == kOpCSum) {
+    if (vec) blasc_kernel<T, F, kOpCSum, true><<<grid, block, 0, s>>>(a);
+    else blasc_kernel<T, F, kOpCSum, false><<<grid, block, 0, s>>>(a);
+  } else if (op == kOpCDotc && sizeof(T) == 8) {
+    if (vec) blasc_kernel<T, F, kOpCDotc, true><<<grid, block, 0, s>>>(a);
+    else blasc_kernel<T, F, kOpCDotc, false><<<grid, block, 0, s>>>(a);
+  } else {
+    return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 
@@ -602,8 +661,11 @@ const void* blas1_kernel_ptr(char type, int op, bool vec) {
   switch (type) {
     case 'd': return real_kernel_ptr<double, F>(op, vec);
     case 's': return real_kernel_ptr<float, F>(op, vec);
-    case 'z': return op == kOpCSum ? (const void*)blasc_kernel<double, F, kOpCSum> : (const void*)blasc_kernel<double, F, kOpCDotc>;
-    default: return (const void*)blasc_kernel<float, F, kOpCSum>;
+    case 'z':
+      if (op == kOpCSum) return vec ? (const void*)blasc_kernel<double, F, kOpCSum, true> : (const void*)blasc_kernel<double, F, kOpCSum, false>;
+      return vec ? (const void*)blasc_kernel<double, F, kOpCDotc, true> : (const void*)blasc_kernel<double, F, kOpCDotc, false>;
+    default:
+      return vec ? (const void*)blasc_kernel<float, F, kOpCSum, true> : (const void*)blasc_kernel<float, F, kOpCSum, false>;
   }
 }
 

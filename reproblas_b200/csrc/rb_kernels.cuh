@@ -47,10 +47,16 @@ cudaError_t launch_blas1_d(int fold, int op, bool vec, int grid, int block,
                            const Blas1Args& a, cudaStream_t s);
 cudaError_t launch_blas1_s(int fold, int op, bool vec, int grid, int block,
                            const Blas1Args& a, cudaStream_t s);
-cudaError_t launch_blas1_z(int fold, int op, int grid, int block, const Blas1Args& a,
+cudaError_t launch_blas1_z(int fold, int op, bool vec, int grid, int block, const Blas1Args& a,
                            cudaStream_t s);
-cudaError_t launch_blas1_c(int fold, int op, int grid, int block, const Blas1Args& a,
+cudaError_t launch_blas1_c(int fold, int op, bool vec, int grid, int block, const Blas1Args& a,
                            cudaStream_t s);
+
+// Complex elements per warp tile of the complex kernels' vector body, for complex elements
+// of `elem` bytes (8 or 16): 32 lanes x 4 (sum) or 2 (dotc) 16-byte vectors.
+__host__ __device__ constexpr int blas1_complex_tile(size_t elem, int op) {
+  return 32 * (op == kOpCSum ? 4 : 2) * (int)(16 / elem);
+}
 
 // out (device double_binned) += each of `count` device double_binned states.
 cudaError_t launch_merge_states(int fold, int count, const double* states, double* out,
@@ -68,8 +74,8 @@ inline size_t blas1_record_bytes(size_t elem, int fold, int comps) {
 struct Blas1FoldOps {
   cudaError_t (*real_d)(int op, bool vec, int grid, int block, const Blas1Args& a, cudaStream_t s);
   cudaError_t (*real_s)(int op, bool vec, int grid, int block, const Blas1Args& a, cudaStream_t s);
-  cudaError_t (*cplx_z)(int op, int grid, int block, const Blas1Args& a, cudaStream_t s);
-  cudaError_t (*cplx_c)(int op, int grid, int block, const Blas1Args& a, cudaStream_t s);
+  cudaError_t (*cplx_z)(int op, bool vec, int grid, int block, const Blas1Args& a, cudaStream_t s);
+  cudaError_t (*cplx_c)(int op, bool vec, int grid, int block, const Blas1Args& a, cudaStream_t s);
   cudaError_t (*merge)(int count, const double* states, double* out, cudaStream_t s);
   const void* (*kernel)(char type, int op, bool vec);
 };

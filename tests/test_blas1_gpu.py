@@ -187,6 +187,36 @@ def test_edge_sizes_strides_alignment(cuda, rb, port, fold):
                 assert same_state(host(z), want, fold), (n, inc, off)
 
 
+@pytest.mark.parametrize("fold", [2, 3, 5, 8])
+def test_complex_edge_sizes_strides_alignment(cuda, rb, port, fold):
+    """Complex sums and dots around the vector body's warp tiles (128 and 256 complex
+    elements), with unit and double strides, and float complex at an odd element offset
+    (an 8-byte head before the 16-byte aligned body)."""
+    sizes = [0, 1, 2, 63, 64, 65, 127, 128, 129, 255, 256, 257, 4095, 4097, 65537]
+    for n in sizes:
+        for inc in (1, 2):
+            for off in (0, 1):
+                bx = gen_complex("loguniform", n * inc + 2, n + 3)
+                by = gen_complex("normal", n * inc + 2, n + 4)
+                X, Y = dev(cuda, bx.view(np.float64)), dev(cuda, by.view(np.float64))
+                xs, ys = bx[off:], by[off:]
+                want = binned_zeros(fold, "z"); port.zbzsum(fold, n, ptr(xs), inc, ptr(want))
+                z = dev(cuda, binned_zeros(fold, "z"))
+                rb.call("binnedBLAS_zbzsum", fold, n, X[2 * off:], inc, z)
+                assert same_bits(host(z), want), ("zsum", n, inc, off)
+                want = binned_zeros(fold, "z")
+                port.zbzdotc(fold, n, ptr(xs), inc, ptr(ys), inc, ptr(want))
+                z = dev(cuda, binned_zeros(fold, "z"))
+                rb.call("binnedBLAS_zbzdotc", fold, n, X[2 * off:], inc, Y[2 * off:], inc, z)
+                assert same_bits(host(z), want), ("zdotc", n, inc, off)
+                bc = bx.astype(np.complex64)
+                want = binned_zeros(fold, "c"); port.cbcsum(fold, n, ptr(bc[off:]), inc, ptr(want))
+                XC = dev(cuda, bc.view(np.float32))
+                z = dev(cuda, binned_zeros(fold, "c"))
+                rb.call("binnedBLAS_cbcsum", fold, n, XC[2 * off:], inc, z)
+                assert same_state(host(z), want, fold, comps=2), ("csum", n, inc, off)
+
+
 def test_accumulate_resume(cuda, rb, port):
     """binnedBLAS_* add into the caller's state: two halves equal the whole."""
     n = 300001
