@@ -53,7 +53,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-secondary", action="store_true",
                    help="skip the dgemm (plain vs int8-sliced) and dgemv measurements")
-    p.add_argument("--profile-kernel", choices=["int8", "plain_gemm", "gemv_n", "gemv_t"],
+    p.add_argument("--profile-kernel", choices=["int8", "plain_gemm", "gemv_n", "gemv_t", "zdotc",
+                                                "zsum", "csum", "dnrm2"],
                    help="only run that kernel `--steps` times on an n^3 (or n^2) case, for ncu")
     p.add_argument("--profile-n", type=int, default=2048)
     p.add_argument("--profile-m", type=int, default=0,
@@ -587,6 +588,26 @@ def profile_case(args):
             rb.call("reproBLAS_rdgemv", 3, "r", ta, m, n, 1.5, A, n, x, 1, 0.5, y, 1)
         torch.cuda.synchronize()
         print("profile case done: %s m=%d n=%d" % (args.profile_kernel, m, n))
+        return
+    if args.profile_kernel in ("zdotc", "zsum", "csum", "dnrm2"):
+        # n elements (complex for the z/c routines), uniform(-1, 1), fold 3
+        k = args.profile_kernel
+        comps = 1 if k == "dnrm2" else 2
+        dt = torch.float32 if k == "csum" else torch.float64
+        X = torch.from_numpy(rng.uniform(-1, 1, comps * n)).to(dt).cuda()
+        Y = torch.from_numpy(rng.uniform(-1, 1, comps * n)).to(dt).cuda()
+        out = torch.zeros(2, dtype=dt, device="cuda")
+        for _ in range(args.warmup + args.steps):
+            if k == "zdotc":
+                rb.call("reproBLAS_rzdotc_sub", 3, n, X, 1, Y, 1, out)
+            elif k == "zsum":
+                rb.call("reproBLAS_rzsum_sub", 3, n, X, 1, out)
+            elif k == "csum":
+                rb.call("reproBLAS_rcsum_sub", 3, n, X, 1, out)
+            else:
+                rb.call("reproBLAS_rdnrm2", 3, n, X, 1)
+        torch.cuda.synchronize()
+        print("profile case done: %s n=%d" % (k, n))
         return
     A = torch.from_numpy(int8_operands(rng, n, n)).cuda()
     B = torch.from_numpy(int8_operands(rng, n, n)).cuda()
