@@ -66,9 +66,11 @@ template <> struct BT<double> {
     return e == 0 ? kMaxIndex : (2046 - e) / 40;
   }
   // Smallest key whose index is below i: (2046 - e) / 40 < i  <=>  e >= 2047 - 40 i.
-  // Zero and subnormal keys (index 51) never are. 0 for the empty state (anything raises).
+  // Zero and subnormal keys (index 51) never are. 0 for the empty state (anything raises)
+  // and for index 0, where no key raises but deposits take the compressed first slice, so
+  // every tile there takes the general path.
   static __device__ __forceinline__ unsigned cap_of(int i) {
-    return i >= kMaxIndex + 1 ? 0u : (unsigned)(2047 - 40 * i) << 20;
+    return (i >= kMaxIndex + 1 || i == 0) ? 0u : (unsigned)(2047 - 40 * i) << 20;
   }
   static __device__ __forceinline__ double compress(double x) { return __dmul_rn(x, 0x1p-14); }
   static __device__ __forceinline__ double half_expand(double m) { return __dmul_rn(m, 0x1p13); }
@@ -113,9 +115,10 @@ template <> struct BT<float> {
   static __device__ __forceinline__ unsigned key(float x) { return __float_as_uint(x) & 0x7fffffffu; }
   static __device__ __forceinline__ int index_of_key(unsigned k) { return index_of_abs(k); }
   // Smallest key whose index is below i for normal magnitudes: e >= 255 - 13 i. Near the
-  // bottom (i >= 19) subnormal indices depend on the leading bit, so every key is checked.
+  // bottom (i >= 19) subnormal indices depend on the leading bit, so every key is checked;
+  // at index 0 (compressed first slice) every tile takes the general path.
   static __device__ __forceinline__ unsigned cap_of(int i) {
-    return i >= 19 ? 0u : (unsigned)(255 - 13 * i) << 23;
+    return (i >= 19 || i == 0) ? 0u : (unsigned)(255 - 13 * i) << 23;
   }
   static __device__ __forceinline__ float compress(float x) { return __fmul_rn(x, 0x1p-12f); }
   static __device__ __forceinline__ float half_expand(float m) { return __fmul_rn(m, 0x1p11f); }
@@ -158,7 +161,8 @@ template <typename T, int F> struct Acc {
   int idx;        // bin index of pri[0], kEmpty if empty
   int deposits;   // deposits since the last renormalisation
   unsigned flags; // non-finite classes seen
-  unsigned cap;   // magnitude keys >= cap may need a coarser index (see BT::cap_of)
+  unsigned cap;   // keys >= cap may need a coarser index, or are non-finite, or the
+                  // accumulator is empty or at index 0 (see BT::cap_of): the general path
 
   __device__ __forceinline__ void set_idx(int i) { idx = i; cap = B::cap_of(i); }
   __device__ __forceinline__ void set_idx_from_pri() {
@@ -270,6 +274,13 @@ template <typename T, int F> struct Acc {
     deposits += n;
   }
 
+  // True when a tile of n values with largest key m can be deposited as is: finite, no
+  // index raise, no renormalisation due, index not 0 (one compare against cap covers the
+  // first three conditions and the last, see BT::cap_of).
+  __device__ __forceinline__ bool fast(unsigned m, int n) const {
+    return m < cap && deposits + n <= B::kEndurance;
+  }
+
   // Deposit K values of which the first nv are real elements (the rest are zeros, whose
   // deposit changes nothing). Non-finite values only record their class.
   template <int K>
@@ -280,6 +291,12 @@ template <typename T, int F> struct Acc {
     for (int k = 0; k < K; k++) {
       unsigned kk = B::key(v[k]);
       m = (k < nv && kk > m) ? kk : m;
+    }
+    if (fast(m, nv)) {
+      deposits += nv;
+#pragma unroll
+      for (int k = 0; k < K; k++) deposit(v[k]);
+      return;
     }
     if (m >= B::kInfKey) {
 #pragma unroll
@@ -359,9 +376,9 @@ template <typename T, int F> struct Acc {
 };
 
 // Deposit K values into each of two accumulators (all K counted as elements; zeros deposit
-// nothing). Same result as a.tile<K>(va, K); b.tile<K>(vb, K), but in the common case (finite
-// values, neither accumulator at index 0) the two deposit chains sit in one straight-line
-// block, so their latencies overlap.
+// nothing). Same result as a.tile<K>(va, K); b.tile<K>(vb, K), but in the common case (both
+// tiles on their fast path) the two deposit chains sit in one straight-line block, so their
+// latencies overlap.
 template <typename T, int F, int K>
 __device__ __forceinline__ void tile2(Acc<T, F>& a, const T (&va)[K], Acc<T, F>& b,
                                       const T (&vb)[K]) {
@@ -373,29 +390,18 @@ __device__ __forceinline__ void tile2(Acc<T, F>& a, const T (&va)[K], Acc<T, F>&
     ma = ka > ma ? ka : ma;
     mb = kb > mb ? kb : mb;
   }
-  if (ma >= B::kInfKey || mb >= B::kInfKey) {
-    a.template tile<K>(va, K);
-    b.template tile<K>(vb, K);
-    return;
-  }
-  a.prepare(ma, K);
-  b.prepare(mb, K);
-  if (a.idx != 0 && b.idx != 0) {
+  if (a.fast(ma, K) && b.fast(mb, K)) {
+    a.deposits += K;
+    b.deposits += K;
 #pragma unroll
     for (int k = 0; k < K; k++) {
       a.deposit(va[k]);
       b.deposit(vb[k]);
     }
-  } else {
-#pragma unroll
-    for (int k = 0; k < K; k++) {
-      if (a.idx == 0) a.deposit0(va[k]); else a.deposit(va[k]);
-    }
-#pragma unroll
-    for (int k = 0; k < K; k++) {
-      if (b.idx == 0) b.deposit0(vb[k]); else b.deposit(vb[k]);
-    }
+    return;
   }
+  a.template tile<K>(va, K);
+  b.template tile<K>(vb, K);
 }
 
 // binned_ddmconv (src/binned/ddmconv.c:23-81): fixed-order conversion to double with
