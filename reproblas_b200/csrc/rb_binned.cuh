@@ -72,6 +72,12 @@ template <> struct BT<double> {
   static __device__ __forceinline__ unsigned cap_of(int i) {
     return (i >= kMaxIndex + 1 || i == 0) ? 0u : (unsigned)(2047 - 40 * i) << 20;
   }
+  // bin(i) / 6, which the conversion (ddmconv.c) forms by division: every bin is 1.5 times
+  // a power of two, so the quotient is the exact power of two a quarter of that one, and
+  // the correctly rounded division returns it unchanged.
+  static __device__ __forceinline__ double bin6(int i) {
+    return from(((bits(bin(i)) >> 52) - 2) << 52);
+  }
   static __device__ __forceinline__ double compress(double x) { return __dmul_rn(x, 0x1p-14); }
   static __device__ __forceinline__ double half_expand(double m) { return __dmul_rn(m, 0x1p13); }
   static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
@@ -119,6 +125,11 @@ template <> struct BT<float> {
   // at index 0 (compressed first slice) every tile takes the general path.
   static __device__ __forceinline__ unsigned cap_of(int i) {
     return (i >= 19 || i == 0) ? 0u : (unsigned)(255 - 13 * i) << 23;
+  }
+  // (double)bin(i) / 6 as the conversion (ssmconv.c) forms it in double: exactly the power
+  // of two a quarter of the bin's (see BT<double>::bin6).
+  static __device__ __forceinline__ double bin6(int i) {
+    return __longlong_as_double((long long)((unsigned long long)((bits(bin(i)) >> 23) + 1023 - 129) << 52));
   }
   static __device__ __forceinline__ float compress(float x) { return __fmul_rn(x, 0x1p-12f); }
   static __device__ __forceinline__ float half_expand(float m) { return __fmul_rn(m, 0x1p11f); }
@@ -420,16 +431,16 @@ __device__ inline double conv(const double* pri, const double* car, int inc) {
     int scaled = F < 3 - X_index ? F : 3 - X_index;
     if (scaled < 0) scaled = 0;
     if (X_index == 0) {
-      Y = __dadd_rn(Y, __dmul_rn(car[0], __dmul_rn(__dmul_rn(__ddiv_rn(B::bin(0), 6.0), sd), 0x1p14)));
-      Y = __dadd_rn(Y, __dmul_rn(car[inc], __dmul_rn(__ddiv_rn(B::bin(1), 6.0), sd)));
+      Y = __dadd_rn(Y, __dmul_rn(car[0], __dmul_rn(__dmul_rn(B::bin6(0), sd), 0x1p14)));
+      Y = __dadd_rn(Y, __dmul_rn(car[inc], __dmul_rn(B::bin6(1), sd)));
       Y = __dadd_rn(Y, __dmul_rn(__dmul_rn(__dsub_rn(pri[0], B::bin(0)), sd), 0x1p14));
       i = 2;
     } else {
-      Y = __dadd_rn(Y, __dmul_rn(car[0], __dmul_rn(__ddiv_rn(B::bin(X_index), 6.0), sd)));
+      Y = __dadd_rn(Y, __dmul_rn(car[0], __dmul_rn(B::bin6(X_index), sd)));
       i = 1;
     }
     for (; i < scaled; i++) {
-      Y = __dadd_rn(Y, __dmul_rn(car[i * inc], __dmul_rn(__ddiv_rn(B::bin(X_index + i), 6.0), sd)));
+      Y = __dadd_rn(Y, __dmul_rn(car[i * inc], __dmul_rn(B::bin6(X_index + i), sd)));
       Y = __dadd_rn(Y, __dmul_rn(__dsub_rn(pri[(i - 1) * inc], B::bin(X_index + i - 1)), sd));
     }
     if (i == F) {
@@ -440,14 +451,14 @@ __device__ inline double conv(const double* pri, const double* car, int inc) {
     if (isinf(t)) return t;
     Y = t;
     for (; i < F; i++) {
-      Y = __dadd_rn(Y, __dmul_rn(car[i * inc], __ddiv_rn(B::bin(X_index + i), 6.0)));
+      Y = __dadd_rn(Y, __dmul_rn(car[i * inc], B::bin6(X_index + i)));
       Y = __dadd_rn(Y, __dsub_rn(pri[(i - 1) * inc], B::bin(X_index + i - 1)));
     }
     Y = __dadd_rn(Y, __dsub_rn(pri[(F - 1) * inc], B::bin(X_index + F - 1)));
   } else {
-    Y = __dadd_rn(Y, __dmul_rn(car[0], __ddiv_rn(B::bin(X_index), 6.0)));
+    Y = __dadd_rn(Y, __dmul_rn(car[0], B::bin6(X_index)));
     for (i = 1; i < F; i++) {
-      Y = __dadd_rn(Y, __dmul_rn(car[i * inc], __ddiv_rn(B::bin(X_index + i), 6.0)));
+      Y = __dadd_rn(Y, __dmul_rn(car[i * inc], B::bin6(X_index + i)));
       Y = __dadd_rn(Y, __dsub_rn(pri[(i - 1) * inc], B::bin(X_index + i - 1)));
     }
     Y = __dadd_rn(Y, __dsub_rn(pri[(F - 1) * inc], B::bin(X_index + F - 1)));
@@ -466,16 +477,16 @@ __device__ inline float sconv(const float* pri, const float* car, int inc) {
   double Y = 0.0;
   int i;
   if (X_index == 0) {
-    Y = __dadd_rn(Y, __dmul_rn(__dmul_rn((double)car[0], __ddiv_rn((double)B::bin(0), 6.0)), 0x1p12));
-    Y = __dadd_rn(Y, __dmul_rn((double)car[inc], __ddiv_rn((double)B::bin(1), 6.0)));
+    Y = __dadd_rn(Y, __dmul_rn(__dmul_rn((double)car[0], B::bin6(0)), 0x1p12));
+    Y = __dadd_rn(Y, __dmul_rn((double)car[inc], B::bin6(1)));
     Y = __dadd_rn(Y, __dmul_rn((double)__fsub_rn(pri[0], B::bin(0)), 0x1p12));
     i = 2;
   } else {
-    Y = __dadd_rn(Y, __dmul_rn((double)car[0], __ddiv_rn((double)B::bin(X_index), 6.0)));
+    Y = __dadd_rn(Y, __dmul_rn((double)car[0], B::bin6(X_index)));
     i = 1;
   }
   for (; i < F; i++) {
-    Y = __dadd_rn(Y, __dmul_rn((double)car[i * inc], __ddiv_rn((double)B::bin(X_index + i), 6.0)));
+    Y = __dadd_rn(Y, __dmul_rn((double)car[i * inc], B::bin6(X_index + i)));
     Y = __dadd_rn(Y, (double)__fsub_rn(pri[(i - 1) * inc], B::bin(X_index + i - 1)));
   }
   Y = __dadd_rn(Y, (double)__fsub_rn(pri[(F - 1) * inc], B::bin(X_index + F - 1)));
