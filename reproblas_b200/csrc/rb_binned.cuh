@@ -415,6 +415,36 @@ __device__ __forceinline__ void tile2(Acc<T, F>& a, const T (&va)[K], Acc<T, F>&
   b.template tile<K>(vb, K);
 }
 
+// Deposit row n of v (K values each) into accumulator n, for N accumulators: tile2 for N
+// of them. When every tile is on its fast path the N deposit chains are interleaved in one
+// straight-line block.
+template <typename T, int F, int K, int N>
+__device__ __forceinline__ void tileN(Acc<T, F> (&a)[N], const T (&v)[N][K]) {
+  using B = BT<T>;
+  bool ok = true;
+#pragma unroll
+  for (int n = 0; n < N; n++) {
+    unsigned m = 0;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const unsigned kk = B::key(v[n][k]);
+      m = kk > m ? kk : m;
+    }
+    ok = ok && a[n].fast(m, K);
+  }
+  if (ok) {
+#pragma unroll
+    for (int n = 0; n < N; n++) a[n].deposits += K;
+#pragma unroll
+    for (int k = 0; k < K; k++)
+#pragma unroll
+      for (int n = 0; n < N; n++) a[n].deposit(v[n][k]);
+    return;
+  }
+#pragma unroll
+  for (int n = 0; n < N; n++) a[n].template tile<K>(v[n], K);
+}
+
 // binned_ddmconv (src/binned/ddmconv.c:23-81): fixed-order conversion to double with
 // scaling when the index is within 3 of the top.
 template <int F>

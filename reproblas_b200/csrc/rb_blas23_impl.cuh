@@ -363,11 +363,9 @@ __device__ __forceinline__ void gemm_tile(const GemmArgs& g, long long m0, long 
   const int tid = threadIdx.x;
   const int tx = tid % Cfg::TX, ty = tid / Cfg::TX;
 
-  Acc<double, F> acc[TM][TN];
+  Acc<double, F> acc[TM * TN];   // entry (i, j) at i * TN + j
 #pragma unroll
-  for (int i = 0; i < TM; i++)
-#pragma unroll
-    for (int j = 0; j < TN; j++) acc[i][j].zero();
+  for (int e = 0; e < TM * TN; e++) acc[e].zero();
 
   const bool a_k_fast = g.sak == 1;   // which stride is unit decides the load order
   const bool b_j_fast = g.sbj == 1;
@@ -399,10 +397,10 @@ __device__ __forceinline__ void gemm_tile(const GemmArgs& g, long long m0, long 
     }
     __syncthreads();
     const int kmax = (g.K - k0) < BK ? (int)(g.K - k0) : BK;
+    // past K both tiles hold zeros, whose products deposit nothing
 #pragma unroll 1
     for (int kk = 0; kk < BK; kk += 4) {
       if (kk >= kmax) break;
-      const int nv = (kmax - kk) < 4 ? (kmax - kk) : 4;
       double av[TM][4], bv[TN][4];
 #pragma unroll
       for (int q = 0; q < 4; q++) {
@@ -411,15 +409,14 @@ __device__ __forceinline__ void gemm_tile(const GemmArgs& g, long long m0, long 
 #pragma unroll
         for (int j = 0; j < TN; j++) bv[j][q] = Bs[kk + q][tx + j * Cfg::TX];
       }
+      double p[TM * TN][4];
 #pragma unroll
       for (int i = 0; i < TM; i++)
 #pragma unroll
-        for (int j = 0; j < TN; j++) {
-          double p[4];
+        for (int j = 0; j < TN; j++)
 #pragma unroll
-          for (int q = 0; q < 4; q++) p[q] = __dmul_rn(av[i][q], bv[j][q]);
-          acc[i][j].template tile<4>(p, nv);
-        }
+          for (int q = 0; q < 4; q++) p[i * TN + j][q] = __dmul_rn(av[i][q], bv[j][q]);
+      tileN<double, F, 4, TM * TN>(acc, p);
     }
     __syncthreads();
   }
@@ -430,9 +427,9 @@ __device__ __forceinline__ void gemm_tile(const GemmArgs& g, long long m0, long 
     for (int j = 0; j < TN; j++) {
       const long long gi = m0 + ty + i * Cfg::TY, gj = n0 + tx + j * Cfg::TX;
       if (gi < g.M && gj < g.N) {
-        acc[i][j].renorm();
+        acc[i * TN + j].renorm();
         const long long off = gi * g.sci + gj * g.scj;
-        finish_entry<F>(acc[i][j], g.mode, g.C + off, g.beta, g.Cbin + off * 2 * F);
+        finish_entry<F>(acc[i * TN + j], g.mode, g.C + off, g.beta, g.Cbin + off * 2 * F);
       }
     }
 }
