@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--no-secondary", action="store_true",
                    help="skip the dgemm (plain vs int8-sliced) and dgemv measurements")
     p.add_argument("--profile-kernel", choices=["int8", "plain_gemm", "gemv_n", "gemv_t", "zdotc",
-                                                "zsum", "csum", "dnrm2"],
+                                                "zsum", "csum", "dnrm2", "batched"],
                    help="only run that kernel `--steps` times on an n^3 (or n^2) case, for ncu")
     p.add_argument("--profile-n", type=int, default=2048)
     p.add_argument("--profile-m", type=int, default=0,
@@ -416,7 +416,7 @@ def blas1_sweep(torch, rb):
     return out
 
 
-def batched_case(torch, rb, rng):
+def batched_case(torch, rb, rng, profile_steps=0, total_log2=28):
     """Batched ragged configuration: 10,000 ddot segments with log-uniform lengths (drawn as
     floor(2^U(0,20)), then scaled so the total is ~2^28 elements, normal values) and 512
     dgemm instances with m, n, k uniform over {16..256}, uniform(-1,1), fold 3; autotuned
@@ -424,7 +424,7 @@ def batched_case(torch, rb, rng):
     import ctypes
     nseg = 10000
     lens = np.floor(np.exp2(rng.uniform(0, 20, nseg)))
-    lens = np.maximum(1, np.floor(lens * (2.0 ** 28 / lens.sum()))).astype(np.int32)
+    lens = np.maximum(1, np.floor(lens * (2.0 ** total_log2 / lens.sum()))).astype(np.int32)
     offs = np.concatenate([[0], np.cumsum(lens.astype(np.int64))[:-1]]).astype(np.int64)
     total = int(lens.astype(np.int64).sum())
     X = torch.from_numpy(rng.standard_normal(total)).cuda()
@@ -448,6 +448,14 @@ def batched_case(torch, rb, rng):
     plan = rb.lib.rb_batch_plan_create(3, nseg, offs.ctypes.data, lens.ctypes.data, X.data_ptr(),
                                        Y.data_ptr(), res.data_ptr(), None, ng, ctypes.addressof(inst))
     rb.check()
+    if profile_steps:
+        # profile case: the default schedule, no autotuning, no timing
+        stream = torch.cuda.current_stream().cuda_stream
+        for _ in range(profile_steps):
+            rb.call("rb_batch_plan_run", plan, stream)
+        torch.cuda.synchronize()
+        rb.lib.rb_batch_plan_destroy(plan)
+        return None
     t0 = time.perf_counter()
     rb.call("rb_batch_plan_autotune", plan, 3)
     tune_s = time.perf_counter() - t0
@@ -464,7 +472,17 @@ def batched_case(torch, rb, rng):
         o, l = int(offs[i]), int(lens[i])
         same &= rb.call("reproBLAS_rddot", 3, l, X[o:], 1, Y[o:], 1) == got[i]
     rb.lib.rb_batch_plan_destroy(plan)
-    return {"ms": round(t * 1e3, 3), "segments": nseg, "segment_elements": total,
+    # the two halves alone (same default schedule each): how much of them one launch overlaps
+    parts = {}
+    for name, ns, ngm in (("segments_only_ms", nseg, 0), ("gemms_only_ms", 0, ng)):
+        p2 = rb.lib.rb_batch_plan_create(3, ns, offs.ctypes.data, lens.ctypes.data, X.data_ptr(),
+                                         Y.data_ptr(), res.data_ptr(), None, ngm,
+                                         ctypes.addressof(inst))
+        rb.check()
+        parts[name] = round(1e3 * _event_time(torch, lambda: rb.call("rb_batch_plan_run", p2, stream),
+                                              5, warm=2), 3)
+        rb.lib.rb_batch_plan_destroy(p2)
+    return {"ms": round(t * 1e3, 3), **parts, "segments": nseg, "segment_elements": total,
             "dgemm_instances": ng, "reduction_gbs": round(16.0 * total / t / 1e9, 1),
             "gemm_tflops_if_alone": round(flops / t / 1e12, 3),
             "schedule": {"tile": [info[0].value, info[1].value], "chunk": info[2].value,
@@ -588,6 +606,11 @@ def profile_case(args):
             rb.call("reproBLAS_rdgemv", 3, "r", ta, m, n, 1.5, A, n, x, 1, 0.5, y, 1)
         torch.cuda.synchronize()
         print("profile case done: %s m=%d n=%d" % (args.profile_kernel, m, n))
+        return
+    if args.profile_kernel == "batched":
+        # a quarter of the benchmark's segment elements (2^26), the same 512 dgemm instances
+        batched_case(torch, rb, rng, profile_steps=args.warmup + args.steps, total_log2=26)
+        print("profile case done: batched")
         return
     if args.profile_kernel in ("zdotc", "zsum", "csum", "dnrm2"):
         # n elements (complex for the z/c routines), uniform(-1, 1), fold 3

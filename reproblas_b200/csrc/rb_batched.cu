@@ -5,7 +5,8 @@
 // reproBLAS_rdsum (or binnedBLAS_dbddot / dbdsum into a given state) on that segment, and
 // each dgemm instance equals reproBLAS_rdgemm on it, bit for bit.
 //
-// Work items (built on the host, fetched dynamically by CTAs through an atomic counter):
+// Work items (built on the host, fetched dynamically by CTAs through an atomic counter; the
+// streaming items and the dgemm tiles are interleaved, each list longest first):
 //   * kItemSmall: up to 8 short segments, one per warp (lane-strided loads, warp butterfly)
 //   * kItemChunk: one chunk of a long segment, reduced by the whole CTA into a record; the
 //     last chunk of a segment to finish (per-segment ticket) merges its records
@@ -374,9 +375,26 @@ bool build_config(rb_batch_plan* p) {
                    [](const std::pair<double, Item>& x, const std::pair<double, Item>& y) {
                      return x.first > y.first;
                    });
+  // Interleave the streaming items (segments: bandwidth-bound) with the dgemm tiles (FP64-
+  // bound), each list longest first, so that the CTAs sharing an SM tend to run one of each:
+  // take next from the list that has progressed less, as a fraction of its total cost.
+  std::vector<std::pair<double, Item>> mem, cmp;
+  double mem_total = 0, cmp_total = 0;
+  for (auto& w : work) {
+    if (w.second.type == kItemTile) { cmp.push_back(w); cmp_total += w.first; }
+    else { mem.push_back(w); mem_total += w.first; }
+  }
   std::vector<Item> items;
   items.reserve(work.size());
-  for (auto& w : work) items.push_back(w.second);
+  size_t im = 0, ic = 0;
+  double mem_done = 0, cmp_done = 0;
+  while (im < mem.size() || ic < cmp.size()) {
+    const bool take_mem =
+        ic >= cmp.size() ||
+        (im < mem.size() && mem_done / (mem_total > 0 ? mem_total : 1) <= cmp_done / (cmp_total > 0 ? cmp_total : 1));
+    if (take_mem) { items.push_back(mem[im].second); mem_done += mem[im].first; im++; }
+    else { items.push_back(cmp[ic].second); cmp_done += cmp[ic].first; ic++; }
+  }
   p->nitems = (int)items.size();
 
   auto up = [](void** dst, const void* src, size_t bytes) {
