@@ -771,6 +771,239 @@ void rbo_cbcsum(int fold, int N, const void *Xv, int incX, float *Y) {
 }
 
 /* ------------------------------------------------------------------------- */
+/* Absolute sums and the remaining complex dots                                */
+/* ------------------------------------------------------------------------- */
+#define NB_DASUM 2048   /* src/binnedBLAS/dmdasum.ccog:36 */
+#define NB_SASUM 512    /* src/binnedBLAS/smsasum.ccog:36 */
+#define NB_ZASUM 1024   /* src/binnedBLAS/dmzasum.ccog:36 */
+#define NB_CASUM 256    /* src/binnedBLAS/smcasum.ccog:36 */
+#define NB_ZDOTU 2048   /* src/binnedBLAS/zmzdotu.ccog:36 */
+#define NB_CDOT 512     /* src/binnedBLAS/cmcdotc.ccog:36, cmcdotu.ccog:36 */
+
+/* src/binnedBLAS/dmdasum.ccog:57-101 (via dbdasum.c:18): dmdsum on |x_i| */
+void rbo_dbdasum(int fold, int N, const double *X, int incX, double *Y) {
+  double *pri = Y, *car = Y + fold;
+  int deposits = 0;
+  for (int i = 0; i < N; i += NB_DASUM) {
+    int nb = imin(N - i, NB_DASUM);
+    const double *x = X + (size_t)i * incX;
+    double amax = 0.0;
+    for (int j = 0; j < nb; j++) amax = dmaxabs(amax, x[(size_t)j * incX]);
+    if (isinf(amax) || isinf(pri[0]))
+      for (int j = 0; j < nb; j++) pri[0] += fabs(x[(size_t)j * incX]);
+    if (isnan(pri[0])) return;
+    if (isinf(pri[0])) continue;
+    if (deposits + nb > DENDURANCE) { rbo_dmrenorm(fold, pri, 1, car, 1); deposits = 0; }
+    rbo_dmdupdate(fold, amax, pri, 1, car, 1);
+    for (int j = 0; j < nb; j++) rbo_dmddeposit(fold, fabs(x[(size_t)j * incX]), pri, 1);
+    deposits += nb;
+  }
+  rbo_dmrenorm(fold, pri, 1, car, 1);
+}
+
+/* src/binnedBLAS/smsasum.ccog (via sbsasum.c) */
+void rbo_sbsasum(int fold, int N, const float *X, int incX, float *Y) {
+  float *pri = Y, *car = Y + fold;
+  int deposits = 0;
+  for (int i = 0; i < N; i += NB_SASUM) {
+    int nb = imin(N - i, NB_SASUM);
+    const float *x = X + (size_t)i * incX;
+    float amax = 0.0f;
+    for (int j = 0; j < nb; j++) amax = smaxabs(amax, x[(size_t)j * incX]);
+    if (isinf(amax) || isinf(pri[0]))
+      for (int j = 0; j < nb; j++) pri[0] += fabsf(x[(size_t)j * incX]);
+    if (isnan(pri[0])) return;
+    if (isinf(pri[0])) continue;
+    if (deposits + nb > SENDURANCE) { rbo_smrenorm(fold, pri, 1, car, 1); deposits = 0; }
+    rbo_smsupdate(fold, amax, pri, 1, car, 1);
+    for (int j = 0; j < nb; j++) rbo_smsdeposit(fold, fabsf(x[(size_t)j * incX]), pri, 1);
+    deposits += nb;
+  }
+  rbo_smrenorm(fold, pri, 1, car, 1);
+}
+
+/* src/binnedBLAS/dmzasum.ccog (via dbzasum.c): |re| and |im| go to the two components of a
+ * temporary complex state whose components share one index (binned_zbdupdate with the
+ * block's largest component magnitude), then both components are merged into Y. */
+void rbo_dbzasum(int fold, int N, const void *Xv, int incX, double *Y) {
+  const double *X = (const double *)Xv;
+  double t[4 * DMAXFOLD] = {0};
+  int deposits = 0;
+  for (int i = 0; i < N; i += NB_ZASUM) {
+    int nb = imin(N - i, NB_ZASUM);
+    const double *x = X + 2 * (size_t)i * incX;
+    double amax = 0.0;
+    for (int j = 0; j < nb; j++) {
+      amax = dmaxabs(amax, x[2 * (size_t)j * incX]);
+      amax = dmaxabs(amax, x[2 * (size_t)j * incX + 1]);
+    }
+    if (isinf(amax) || isinf(Y[0]))
+      for (int j = 0; j < nb; j++) {
+        Y[0] += fabs(x[2 * (size_t)j * incX]);
+        Y[0] += fabs(x[2 * (size_t)j * incX + 1]);
+      }
+    if (isnan(Y[0]) || isnan(t[0]) || isnan(t[1])) { Y[0] += t[0] + t[1]; return; }
+    if (isinf(Y[0])) continue;
+    if (deposits + nb > DENDURANCE) { zrenorm(fold, t); deposits = 0; }
+    rbo_dmdupdate(fold, amax, t, 2, t + 2 * fold, 2);
+    rbo_dmdupdate(fold, amax, t + 1, 2, t + 2 * fold + 1, 2);
+    for (int j = 0; j < nb; j++) {
+      zdeposit_component(fold, fabs(x[2 * (size_t)j * incX]), t);
+      zdeposit_component(fold, fabs(x[2 * (size_t)j * incX + 1]), t + 1);
+    }
+    deposits += nb;
+  }
+  zrenorm(fold, t);
+  rbo_dmdmadd(fold, t, 2, t + 2 * fold, 2, Y, 1, Y + fold, 1);
+  rbo_dmdmadd(fold, t + 1, 2, t + 2 * fold + 1, 2, Y, 1, Y + fold, 1);
+}
+
+/* src/binnedBLAS/smcasum.ccog (via sbcasum.c): the float form of dmzasum */
+void rbo_sbcasum(int fold, int N, const void *Xv, int incX, float *Y) {
+  const float *X = (const float *)Xv;
+  float t[4 * SMAXFOLD] = {0};
+  int deposits = 0;
+  for (int i = 0; i < N; i += NB_CASUM) {
+    int nb = imin(N - i, NB_CASUM);
+    const float *x = X + 2 * (size_t)i * incX;
+    float amax = 0.0f;
+    for (int j = 0; j < nb; j++) {
+      amax = smaxabs(amax, x[2 * (size_t)j * incX]);
+      amax = smaxabs(amax, x[2 * (size_t)j * incX + 1]);
+    }
+    if (isinf(amax) || isinf(Y[0]))
+      for (int j = 0; j < nb; j++) {
+        Y[0] += fabsf(x[2 * (size_t)j * incX]);
+        Y[0] += fabsf(x[2 * (size_t)j * incX + 1]);
+      }
+    if (isnan(Y[0]) || isnan(t[0]) || isnan(t[1])) { Y[0] += t[0] + t[1]; return; }
+    if (isinf(Y[0])) continue;
+    if (deposits + nb > SENDURANCE) { crenorm(fold, t); deposits = 0; }
+    rbo_smsupdate(fold, amax, t, 2, t + 2 * fold, 2);
+    rbo_smsupdate(fold, amax, t + 1, 2, t + 2 * fold + 1, 2);
+    for (int j = 0; j < nb; j++) {
+      cdeposit_component(fold, fabsf(x[2 * (size_t)j * incX]), t);
+      cdeposit_component(fold, fabsf(x[2 * (size_t)j * incX + 1]), t + 1);
+    }
+    deposits += nb;
+  }
+  crenorm(fold, t);
+  rbo_smsmadd(fold, t, 2, t + 2 * fold, 2, Y, 1, Y + fold, 1);
+  rbo_smsmadd(fold, t + 1, 2, t + 2 * fold + 1, 2, Y, 1, Y + fold, 1);
+}
+
+/* src/binnedBLAS/zmzdotu.ccog:58-120 (via zbzdotu.c): x*y without conjugation. The real part
+ * receives fl(xr*yr) and -fl(xi*yi), the imaginary part fl(xi*yr) and fl(xr*yi), each
+ * deposited separately (depositDotU.py:14-24); endurance halved as for dotc. */
+void rbo_zbzdotu(int fold, int N, const void *Xv, int incX, const void *Yv, int incY,
+                 double *Z) {
+  const double *X = (const double *)Xv, *Yp = (const double *)Yv;
+  double *pri = Z, *car = Z + 2 * fold;
+  int deposits = 0;
+  for (int i = 0; i < N; i += NB_ZDOTU) {
+    int nb = imin(N - i, NB_ZDOTU);
+    const double *x = X + 2 * (size_t)i * incX, *y = Yp + 2 * (size_t)i * incY;
+    double amaxm[2] = {0.0, 0.0};
+    for (int j = 0; j < nb; j++) {
+      double xr = x[2 * (size_t)j * incX], xi = x[2 * (size_t)j * incX + 1];
+      double yr = y[2 * (size_t)j * incY], yi = y[2 * (size_t)j * incY + 1];
+      amaxm[0] = dmaxabs(amaxm[0], xr * yr);
+      amaxm[1] = dmaxabs(amaxm[1], xi * yr);
+      amaxm[0] = dmaxabs(amaxm[0], xi * yi);
+      amaxm[1] = dmaxabs(amaxm[1], xr * yi);
+    }
+    if (isinf(amaxm[0]) || isinf(pri[0]))
+      for (int j = 0; j < nb; j++)
+        pri[0] += x[2 * (size_t)j * incX] * y[2 * (size_t)j * incY] -
+                  x[2 * (size_t)j * incX + 1] * y[2 * (size_t)j * incY + 1];
+    if (isinf(amaxm[1]) || isinf(pri[1]))
+      for (int j = 0; j < nb; j++)
+        pri[1] += x[2 * (size_t)j * incX] * y[2 * (size_t)j * incY + 1] +
+                  x[2 * (size_t)j * incX + 1] * y[2 * (size_t)j * incY];
+    if (isnan(pri[0]) && isnan(pri[1])) return;
+    if (isinf(pri[0]) && isinf(pri[1])) continue;
+    if (dnonfinite(pri[0])) amaxm[0] = pri[0];
+    if (dnonfinite(pri[1])) amaxm[1] = pri[1];
+    if (deposits + nb > DENDURANCE / 2) { zrenorm(fold, Z); deposits = 0; }
+    rbo_dmdupdate(fold, amaxm[0], pri, 2, car, 2);
+    rbo_dmdupdate(fold, amaxm[1], pri + 1, 2, car + 1, 2);
+    for (int j = 0; j < nb; j++) {
+      double xr = x[2 * (size_t)j * incX], xi = x[2 * (size_t)j * incX + 1];
+      double yr = y[2 * (size_t)j * incY], yi = y[2 * (size_t)j * incY + 1];
+      zdeposit_component(fold, xr * yr, pri);
+      zdeposit_component(fold, xi * yr, pri + 1);
+      zdeposit_component(fold, -(xi * yi), pri);
+      zdeposit_component(fold, xr * yi, pri + 1);
+    }
+    if (isinf(amaxm[0])) pri[0] = amaxm[0];
+    if (isinf(amaxm[1])) pri[1] = amaxm[1];
+    deposits += nb;
+  }
+  zrenorm(fold, Z);
+}
+
+/* src/binnedBLAS/cmcdotc.ccog and cmcdotu.ccog (via cbcdotc.c, cbcdotu.c): the float forms
+ * of zmzdotc / zmzdotu (conj = 1 for dotc). */
+static void cbcdot(int conj, int fold, int N, const void *Xv, int incX, const void *Yv,
+                   int incY, float *Z) {
+  const float *X = (const float *)Xv, *Yp = (const float *)Yv;
+  float *pri = Z, *car = Z + 2 * fold;
+  int deposits = 0;
+  for (int i = 0; i < N; i += NB_CDOT) {
+    int nb = imin(N - i, NB_CDOT);
+    const float *x = X + 2 * (size_t)i * incX, *y = Yp + 2 * (size_t)i * incY;
+    float amaxm[2] = {0.0f, 0.0f};
+    for (int j = 0; j < nb; j++) {
+      float xr = x[2 * (size_t)j * incX], xi = x[2 * (size_t)j * incX + 1];
+      float yr = y[2 * (size_t)j * incY], yi = y[2 * (size_t)j * incY + 1];
+      amaxm[0] = smaxabs(amaxm[0], xr * yr);
+      amaxm[1] = smaxabs(amaxm[1], xi * yr);
+      amaxm[0] = smaxabs(amaxm[0], xi * yi);
+      amaxm[1] = smaxabs(amaxm[1], xr * yi);
+    }
+    if (isinf(amaxm[0]) || isinf(pri[0]))
+      for (int j = 0; j < nb; j++) {
+        float xr = x[2 * (size_t)j * incX], xi = x[2 * (size_t)j * incX + 1];
+        float yr = y[2 * (size_t)j * incY], yi = y[2 * (size_t)j * incY + 1];
+        pri[0] += conj ? xr * yr + xi * yi : xr * yr - xi * yi;
+      }
+    if (isinf(amaxm[1]) || isinf(pri[1]))
+      for (int j = 0; j < nb; j++) {
+        float xr = x[2 * (size_t)j * incX], xi = x[2 * (size_t)j * incX + 1];
+        float yr = y[2 * (size_t)j * incY], yi = y[2 * (size_t)j * incY + 1];
+        pri[1] += conj ? xr * yi - xi * yr : xr * yi + xi * yr;
+      }
+    if (isnan(pri[0]) && isnan(pri[1])) return;
+    if (isinf(pri[0]) && isinf(pri[1])) continue;
+    if (fnonfinite(pri[0])) amaxm[0] = pri[0];
+    if (fnonfinite(pri[1])) amaxm[1] = pri[1];
+    rbo_smsupdate(fold, amaxm[0], pri, 2, car, 2);
+    rbo_smsupdate(fold, amaxm[1], pri + 1, 2, car + 1, 2);
+    for (int j = 0; j < nb; j++) {
+      float xr = x[2 * (size_t)j * incX], xi = x[2 * (size_t)j * incX + 1];
+      float yr = y[2 * (size_t)j * incY], yi = y[2 * (size_t)j * incY + 1];
+      /* each component takes two deposits per element: renormalise within the endurance */
+      if (deposits + 2 > SENDURANCE) { crenorm(fold, Z); deposits = 0; }
+      deposits += 2;
+      cdeposit_component(fold, xr * yr, pri);
+      cdeposit_component(fold, conj ? -(xi * yr) : xi * yr, pri + 1);
+      cdeposit_component(fold, conj ? xi * yi : -(xi * yi), pri);
+      cdeposit_component(fold, xr * yi, pri + 1);
+    }
+    if (isinf(amaxm[0])) pri[0] = amaxm[0];
+    if (isinf(amaxm[1])) pri[1] = amaxm[1];
+  }
+  crenorm(fold, Z);
+}
+
+void rbo_cbcdotc(int fold, int N, const void *X, int incX, const void *Y, int incY, float *Z) {
+  cbcdot(1, fold, N, X, incX, Y, incY, Z);
+}
+void rbo_cbcdotu(int fold, int N, const void *X, int incX, const void *Y, int incY, float *Z) {
+  cbcdot(0, fold, N, X, incX, Y, incY, Z);
+}
+
+/* ------------------------------------------------------------------------- */
 /* BLAS2/3: src/binnedBLAS/dbdgemv.ccog:57-162, dbdgemm.ccog:61-420            */
 /* ------------------------------------------------------------------------- */
 static int is_row_major(char o) { return o == 'r' || o == 'R'; }
@@ -893,6 +1126,56 @@ void rbo_rcsum_sub(int fold, int N, const void *X, int incX, void *sum) {  /* rc
   rbo_cbcsum(fold, N, X, incX, acc);
   ((float *)sum)[0] = rbo_ssmconv(fold, acc, 2, acc + 2 * fold, 2);
   ((float *)sum)[1] = rbo_ssmconv(fold, acc + 1, 2, acc + 2 * fold + 1, 2);
+}
+
+double rbo_rdasum(int fold, int N, const double *X, int incX) {            /* rdasum.c */
+  double acc[2 * DMAXFOLD] = {0};
+  rbo_dbdasum(fold, N, X, incX, acc);
+  return rbo_ddmconv(fold, acc, 1, acc + fold, 1);
+}
+
+float rbo_rsasum(int fold, int N, const float *X, int incX) {               /* rsasum.c */
+  float acc[2 * SMAXFOLD] = {0};
+  rbo_sbsasum(fold, N, X, incX, acc);
+  return rbo_ssmconv(fold, acc, 1, acc + fold, 1);
+}
+
+double rbo_rdzasum(int fold, int N, const void *X, int incX) {              /* rdzasum.c */
+  double acc[2 * DMAXFOLD] = {0};
+  rbo_dbzasum(fold, N, X, incX, acc);
+  return rbo_ddmconv(fold, acc, 1, acc + fold, 1);
+}
+
+float rbo_rscasum(int fold, int N, const void *X, int incX) {               /* rscasum.c */
+  float acc[2 * SMAXFOLD] = {0};
+  rbo_sbcasum(fold, N, X, incX, acc);
+  return rbo_ssmconv(fold, acc, 1, acc + fold, 1);
+}
+
+void rbo_rzdotu_sub(int fold, int N, const void *X, int incX, const void *Y, int incY,
+                    void *dotu) {                                   /* rzdotu_sub.c */
+  double acc[4 * DMAXFOLD] = {0};
+  rbo_zbzdotu(fold, N, X, incX, Y, incY, acc);
+  zconv(fold, acc, (double *)dotu);
+}
+
+static void cconv(int fold, const float *acc, float *out) {
+  out[0] = rbo_ssmconv(fold, acc, 2, acc + 2 * fold, 2);
+  out[1] = rbo_ssmconv(fold, acc + 1, 2, acc + 2 * fold + 1, 2);
+}
+
+void rbo_rcdotc_sub(int fold, int N, const void *X, int incX, const void *Y, int incY,
+                    void *dotc) {                                   /* rcdotc_sub.c */
+  float acc[4 * SMAXFOLD] = {0};
+  rbo_cbcdotc(fold, N, X, incX, Y, incY, acc);
+  cconv(fold, acc, (float *)dotc);
+}
+
+void rbo_rcdotu_sub(int fold, int N, const void *X, int incX, const void *Y, int incY,
+                    void *dotu) {                                   /* rcdotu_sub.c */
+  float acc[4 * SMAXFOLD] = {0};
+  rbo_cbcdotu(fold, N, X, incX, Y, incY, acc);
+  cconv(fold, acc, (float *)dotu);
 }
 
 /* rdgemv.c:35-87: y <- conv(binned(beta*y) + sum_j A_ij*(alpha*x_j)) */

@@ -64,6 +64,13 @@ void   rbo_sbsdot(int fold, int N, const float *X, int incX, const float *Y, int
 void   rbo_zbzsum(int fold, int N, const void *X, int incX, double *Y);
 void   rbo_zbzdotc(int fold, int N, const void *X, int incX, const void *Y, int incY, double *Z);
 void   rbo_cbcsum(int fold, int N, const void *X, int incX, float *Y);
+void   rbo_dbdasum(int fold, int N, const double *X, int incX, double *Y);
+void   rbo_sbsasum(int fold, int N, const float *X, int incX, float *Y);
+void   rbo_dbzasum(int fold, int N, const void *X, int incX, double *Y);
+void   rbo_sbcasum(int fold, int N, const void *X, int incX, float *Y);
+void   rbo_zbzdotu(int fold, int N, const void *X, int incX, const void *Y, int incY, double *Z);
+void   rbo_cbcdotc(int fold, int N, const void *X, int incX, const void *Y, int incY, float *Z);
+void   rbo_cbcdotu(int fold, int N, const void *X, int incX, const void *Y, int incY, float *Z);
 void   rbo_dbdgemv(int fold, char Order, char TransA, int M, int N, double alpha,
                    const double *A, int lda, const double *X, int incX, double *Y, int incY);
 void   rbo_dbdgemm(int fold, char Order, char TransA, char TransB, int M, int N, int K,
@@ -79,6 +86,13 @@ float  rbo_rsdot(int fold, int N, const float *X, int incX, const float *Y, int 
 void   rbo_rzsum_sub(int fold, int N, const void *X, int incX, void *sum);
 void   rbo_rzdotc_sub(int fold, int N, const void *X, int incX, const void *Y, int incY, void *dotc);
 void   rbo_rcsum_sub(int fold, int N, const void *X, int incX, void *sum);
+double rbo_rdasum(int fold, int N, const double *X, int incX);
+float  rbo_rsasum(int fold, int N, const float *X, int incX);
+double rbo_rdzasum(int fold, int N, const void *X, int incX);
+float  rbo_rscasum(int fold, int N, const void *X, int incX);
+void   rbo_rzdotu_sub(int fold, int N, const void *X, int incX, const void *Y, int incY, void *dotu);
+void   rbo_rcdotc_sub(int fold, int N, const void *X, int incX, const void *Y, int incY, void *dotc);
+void   rbo_rcdotu_sub(int fold, int N, const void *X, int incX, const void *Y, int incY, void *dotu);
 void   rbo_rdgemv(int fold, char Order, char TransA, int M, int N, double alpha,
                   const double *A, int lda, const double *X, int incX,
                   double beta, double *Y, int incY);

@@ -30,6 +30,20 @@ _SIGS = {
     "zbzsum": (None, [c_int, c_int, c_vp, c_int, c_vp]),
     "zbzdotc": (None, [c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp]),
     "cbcsum": (None, [c_int, c_int, c_vp, c_int, c_vp]),
+    "dbdasum": (None, [c_int, c_int, c_vp, c_int, c_vp]),
+    "sbsasum": (None, [c_int, c_int, c_vp, c_int, c_vp]),
+    "dbzasum": (None, [c_int, c_int, c_vp, c_int, c_vp]),
+    "sbcasum": (None, [c_int, c_int, c_vp, c_int, c_vp]),
+    "zbzdotu": (None, [c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp]),
+    "cbcdotc": (None, [c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp]),
+    "cbcdotu": (None, [c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp]),
+    "rdasum": (c_double, [c_int, c_int, c_vp, c_int]),
+    "rsasum": (c_float, [c_int, c_int, c_vp, c_int]),
+    "rdzasum": (c_double, [c_int, c_int, c_vp, c_int]),
+    "rscasum": (c_float, [c_int, c_int, c_vp, c_int]),
+    "rzdotu_sub": (None, [c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp]),
+    "rcdotc_sub": (None, [c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp]),
+    "rcdotu_sub": (None, [c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp]),
     "dbdgemv": (None, [c_int, c_char, c_char, c_int, c_int, c_double, c_vp, c_int, c_vp, c_int,
                        c_vp, c_int]),
     "dbdgemm": (None, [c_int, c_char, c_char, c_char, c_int, c_int, c_int, c_double, c_vp, c_int,
@@ -68,6 +82,13 @@ _REF_NAMES = {
     "rssum": "reproBLAS_rssum", "rsdot": "reproBLAS_rsdot", "rzsum_sub": "reproBLAS_rzsum_sub",
     "rzdotc_sub": "reproBLAS_rzdotc_sub", "rcsum_sub": "reproBLAS_rcsum_sub",
     "rdgemv": "reproBLAS_rdgemv", "rdgemm": "reproBLAS_rdgemm",
+    "dbdasum": "binnedBLAS_dbdasum", "sbsasum": "binnedBLAS_sbsasum",
+    "dbzasum": "binnedBLAS_dbzasum", "sbcasum": "binnedBLAS_sbcasum",
+    "zbzdotu": "binnedBLAS_zbzdotu", "cbcdotc": "binnedBLAS_cbcdotc",
+    "cbcdotu": "binnedBLAS_cbcdotu", "rdasum": "reproBLAS_rdasum", "rsasum": "reproBLAS_rsasum",
+    "rdzasum": "reproBLAS_rdzasum", "rscasum": "reproBLAS_rscasum",
+    "rzdotu_sub": "reproBLAS_rzdotu_sub", "rcdotc_sub": "reproBLAS_rcdotc_sub",
+    "rcdotu_sub": "reproBLAS_rcdotu_sub",
     "dbdbadd": "binned_dbdbadd", "dbdconv": "binned_dbdconv", "ddbconv": "binned_ddbconv",
     "dbdbaddsq": "binned_dbdbaddsq", "dbbound": "binned_dbbound", "dscale": "binned_dscale",
     "dindex": "binned_dindex", "sindex": "binned_sindex", "sbsbadd": "binned_sbsbadd",

@@ -32,6 +32,25 @@ def hexb(a):
     return np.ascontiguousarray(a).tobytes().hex()
 
 
+def ref_chunked(fn, fold, n, x, y, chunk=256):
+    """The reference's float complex dot applied to consecutive calls of `chunk` elements
+    accumulating into one state."""
+    z = binned_zeros(fold, "c")
+    for o in range(0, n, chunk):
+        m = min(chunk, n - o)
+        fn(fold, m, ptr(x[o:]), 1, ptr(y[o:]), 1, ptr(z))
+    return z
+
+
+def cconv(R, fold, z):
+    """binned_ccbconv_sub through the reference's float conversion of each component."""
+    out = np.zeros(2, np.float32)
+    for k in range(2):
+        comp = np.concatenate([z[k:2 * fold:2], z[2 * fold + k::2]]).astype(np.float32)
+        out[k] = R.ssbconv(fold, ptr(comp))
+    return out
+
+
 def main():
     R = ref()
     if R is None:
@@ -68,6 +87,37 @@ def main():
                 z = binned_zeros(fold, "c"); R.cbcsum(fold, n, ptr(xc), 1, ptr(z)); c["cbcsum"] = hexb(z)
                 o = np.zeros(2, np.float32); R.rcsum_sub(fold, n, ptr(xc), 1, ptr(o)); c["rcsum"] = hexb(o)
                 cases.append(c)
+
+    # Absolute sums and the remaining complex dots, same inputs (plus the float complex y)
+    more = []
+    for dist in DISTS:
+        for n in NS:
+            x = gen(dist, n, 11)
+            xf = gen(dist, n, 11, np.float32)
+            xz, yz = gen_complex(dist, n, 11), gen_complex(dist, n, 12)
+            xc, yc = gen_complex(dist, n, 11, np.complex64), gen_complex(dist, n, 12, np.complex64)
+            hashes = {"x": h(x), "xf": h(xf), "xz": h(xz), "yz": h(yz), "xc": h(xc), "yc": h(yc)}
+            for fold in FOLDS:
+                c = {"dist": dist, "n": n, "fold": fold, "hash": hashes}
+                z = binned_zeros(fold); R.dbdasum(fold, n, ptr(x), 1, ptr(z)); c["dbdasum"] = hexb(z)
+                c["rdasum"] = hexb(np.float64(R.rdasum(fold, n, ptr(x), 1)))
+                z = binned_zeros(fold, "s"); R.sbsasum(fold, n, ptr(xf), 1, ptr(z)); c["sbsasum"] = hexb(z)
+                c["rsasum"] = hexb(np.float32(R.rsasum(fold, n, ptr(xf), 1)))
+                z = binned_zeros(fold); R.dbzasum(fold, n, ptr(xz), 1, ptr(z)); c["dbzasum"] = hexb(z)
+                c["rdzasum"] = hexb(np.float64(R.rdzasum(fold, n, ptr(xz), 1)))
+                z = binned_zeros(fold, "s"); R.sbcasum(fold, n, ptr(xc), 1, ptr(z)); c["sbcasum"] = hexb(z)
+                c["rscasum"] = hexb(np.float32(R.rscasum(fold, n, ptr(xc), 1)))
+                z = binned_zeros(fold, "z"); R.zbzdotu(fold, n, ptr(xz), 1, ptr(yz), 1, ptr(z)); c["zbzdotu"] = hexb(z)
+                o = np.zeros(2); R.rzdotu_sub(fold, n, ptr(xz), 1, ptr(yz), 1, ptr(o)); c["rzdotu"] = hexb(o)
+                # float complex dots: the reference deposits 1024 values per component between
+                # renormalisations in its 512-element blocks, twice the FP32 endurance, and its
+                # state then depends on where a call starts; within 256-element calls it is the
+                # canonical state that any correct order produces, which is what is stored
+                for nm, fn in (("cbcdotc", R.cbcdotc), ("cbcdotu", R.cbcdotu)):
+                    z = ref_chunked(fn, fold, n, xc, yc)
+                    c[nm] = hexb(z)
+                    c["r" + nm[3:]] = hexb(cconv(R, fold, z))
+                more.append(c)
 
     # The dsum configuration quoted by the benchmark: N = 2^20, fold 3, sine and uniform
     cfg0 = []
@@ -123,7 +173,8 @@ def main():
 
     out = {"generator": "tests/golden/make_golden.py", "reference": "ReproBLAS v2.1.0 "
            "compiled by oracle/Makefile (gcc -std=c99 -O3 -march=x86-64-v3)",
-           "blas1": cases, "dsum_config": cfg0, "special": special, "blas23": blas23}
+           "blas1": cases, "blas1_more": more, "dsum_config": cfg0, "special": special,
+           "blas23": blas23}
     with open(os.path.join(HERE, "reference_golden.json"), "w") as f:
         json.dump(out, f, separators=(",", ":"))
     print("wrote", len(cases), "blas1 cases,", len(special), "special,", len(blas23), "blas2/3")

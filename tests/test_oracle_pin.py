@@ -177,3 +177,124 @@ def test_port_against_reference_committed_vectors(port):
     # v2.1.0 reproduces most of the stored FP64 scalar results (the rest predate it)
     print("reference committed vectors reproduced by v2.1.0: %d / %d" % (matched, total))
     assert total > 0 and matched >= total * 0.75, (matched, total)
+
+
+@needs_ref
+@pytest.mark.parametrize("inc", [1, 2])
+def test_port_matches_reference_live_asum_dots(port, inc):
+    """Absolute sums (real and complex, both precisions) and the complex dots (zdotu, cdotc,
+    cdotu): states accumulated into non-empty ones and converted results."""
+    R = ref()
+    rng = np.random.default_rng(123)
+    for trial in range(30):
+        n = int(rng.integers(0, 5000))
+        fold = int(rng.integers(2, 9))
+        dist = ["uniform", "normal", "loguniform", "illcond", "huge", "tiny"][trial % 6]
+        x = gen(dist, n * inc + 1, trial)
+        xf = gen(dist, n * inc + 1, trial, np.float32)
+        xz, yz = gen_complex(dist, n * inc + 1, trial), gen_complex(dist, n * inc + 1, trial + 7)
+        xc = gen_complex(dist, n * inc + 1, trial, np.complex64)
+        yc = gen_complex(dist, n * inc + 1, trial + 7, np.complex64)
+        pre = gen("normal", 5, trial)
+        pref = pre.astype(np.float32)
+        for name, kind, args in [("dbdasum", "d", (x,)), ("sbsasum", "s", (xf,)),
+                                 ("dbzasum", "d", (xz,)), ("sbcasum", "s", (xc,)),
+                                 ("zbzdotu", "z", (xz, yz))]:
+            za = binned_zeros(fold, kind); zb = binned_zeros(fold, kind)
+            if kind in "ds":
+                seed = pre if kind == "d" else pref
+                f = port.dbdsum if kind == "d" else port.sbssum
+                g = R.dbdsum if kind == "d" else R.sbssum
+                f(fold, 5, ptr(seed), 1, ptr(za)); g(fold, 5, ptr(seed), 1, ptr(zb))
+            call_args = []
+            for a in args:
+                call_args += [ptr(a), inc]
+            getattr(port, name)(fold, n, *call_args, ptr(za))
+            getattr(R, name)(fold, n, *call_args, ptr(zb))
+            assert same_state(za, zb, fold, 1 if kind in "ds" else 2), (name, n, fold, dist, inc)
+        assert same_value(port.rdasum(fold, n, ptr(x), inc), R.rdasum(fold, n, ptr(x), inc))
+        assert same_value(port.rsasum(fold, n, ptr(xf), inc), R.rsasum(fold, n, ptr(xf), inc))
+        assert same_value(port.rdzasum(fold, n, ptr(xz), inc), R.rdzasum(fold, n, ptr(xz), inc))
+        assert same_value(port.rscasum(fold, n, ptr(xc), inc), R.rscasum(fold, n, ptr(xc), inc))
+        oa = np.zeros(2); ob = np.zeros(2)
+        port.rzdotu_sub(fold, n, ptr(xz), inc, ptr(yz), inc, ptr(oa))
+        R.rzdotu_sub(fold, n, ptr(xz), inc, ptr(yz), inc, ptr(ob))
+        assert same_value(oa, ob), ("rzdotu", n, fold, dist)
+        # float complex dots: against the reference in calls of at most 256 elements (its
+        # 512-element blocks take twice the FP32 endurance per component, so a whole call can
+        # leave the canonical state; split into such calls it cannot)
+        for name in ("cbcdotc", "cbcdotu"):
+            za = binned_zeros(fold, "c")
+            getattr(port, name)(fold, n, ptr(xc), inc, ptr(yc), inc, ptr(za))
+            zb = binned_zeros(fold, "c")
+            for o in range(0, n, 256):
+                m = min(256, n - o)
+                getattr(R, name)(fold, m, ptr(xc[o * inc:]), inc, ptr(yc[o * inc:]), inc, ptr(zb))
+            assert same_state(za, zb, fold, 2), (name, n, fold, dist, inc)
+
+
+@needs_ref
+def test_port_matches_reference_asum_dots_special_values(port):
+    R = ref()
+    rng = np.random.default_rng(8)
+    for trial in range(200):
+        n = int(rng.integers(1, 3000))
+        x = rng.uniform(-1, 1, n)
+        for _ in range(int(rng.integers(1, 4))):
+            x[int(rng.integers(0, n))] = rng.choice([np.inf, -np.inf, np.nan])
+        assert same_value(port.rdasum(3, n, ptr(x), 1), R.rdasum(3, n, ptr(x), 1))
+        xz = np.empty(n, np.complex128)
+        xz.real = x
+        xz.imag = np.roll(x, 5)
+        yz = np.empty(n, np.complex128)
+        yz.real = rng.uniform(-1, 1, n)
+        yz.imag = rng.uniform(-1, 1, n)
+        assert same_value(port.rdzasum(3, n, ptr(xz), 1), R.rdzasum(3, n, ptr(xz), 1))
+        oa = np.zeros(2); ob = np.zeros(2)
+        port.rzdotu_sub(3, n, ptr(xz), 1, ptr(yz), 1, ptr(oa)); R.rzdotu_sub(3, n, ptr(xz), 1, ptr(yz), 1, ptr(ob))
+        assert same_value(oa, ob)
+        xc, yc = xz.astype(np.complex64), yz.astype(np.complex64)
+        for name in ("cbcdotc", "cbcdotu"):
+            za = binned_zeros(3, "c"); zb = binned_zeros(3, "c")
+            getattr(port, name)(3, n, ptr(xc), 1, ptr(yc), 1, ptr(za))
+            for o in range(0, n, 256):
+                getattr(R, name)(3, min(256, n - o), ptr(xc[o:]), 1, ptr(yc[o:]), 1, ptr(zb))
+            assert same_state(za, zb, 3, 2), name
+
+
+def test_port_matches_golden_asum_dots(port, golden):
+    bad = []
+    for c in golden["blas1_more"]:
+        dist, n, fold = c["dist"], c["n"], c["fold"]
+        x, xf = gen(dist, n, 11), gen(dist, n, 11, np.float32)
+        xz, yz = gen_complex(dist, n, 11), gen_complex(dist, n, 12)
+        xc, yc = gen_complex(dist, n, 11, np.complex64), gen_complex(dist, n, 12, np.complex64)
+        for k, v in {"x": x, "xf": xf, "xz": xz, "yz": yz, "xc": xc, "yc": yc}.items():
+            assert _h(v) == c["hash"][k], "input generator changed for %s" % k
+        key = (dist, n, fold)
+        for name, kind, args, comps in [("dbdasum", "d", (x,), 1), ("sbsasum", "s", (xf,), 1),
+                                        ("dbzasum", "d", (xz,), 1), ("sbcasum", "s", (xc,), 1),
+                                        ("zbzdotu", "z", (xz, yz), 2), ("cbcdotc", "c", (xc, yc), 2),
+                                        ("cbcdotu", "c", (xc, yc), 2)]:
+            z = binned_zeros(fold, kind)
+            call = []
+            for a in args:
+                call += [ptr(a), 1]
+            getattr(port, name)(fold, n, *call, ptr(z))
+            dt = np.float64 if kind in "dz" else np.float32
+            if not same_state(z, from_hex(c[name], dt), fold, comps):
+                bad.append((name, key))
+        for name, dt, val in [("rdasum", np.float64, port.rdasum(fold, n, ptr(x), 1)),
+                              ("rsasum", np.float32, port.rsasum(fold, n, ptr(xf), 1)),
+                              ("rdzasum", np.float64, port.rdzasum(fold, n, ptr(xz), 1)),
+                              ("rscasum", np.float32, port.rscasum(fold, n, ptr(xc), 1))]:
+            if not same_value(np.asarray(val, dt), from_hex(c[name], dt)[0]):
+                bad.append((name, key))
+        for name, fn, dt, a, b in [("rzdotu", port.rzdotu_sub, np.float64, xz, yz),
+                                   ("rdotc", port.rcdotc_sub, np.float32, xc, yc),
+                                   ("rdotu", port.rcdotu_sub, np.float32, xc, yc)]:
+            o = np.zeros(2, dt)
+            fn(fold, n, ptr(a), 1, ptr(b), 1, ptr(o))
+            if not same_value(o, from_hex(c[name], dt)):
+                bad.append((name, key))
+    assert not bad, bad[:10]
