@@ -406,6 +406,11 @@ def blas1_sweep(torch, rb):
         "zsum": (16.0 * nc, lambda: rb.call("binnedBLAS_zbzsum", FOLD, nc, x, 1, zc)),
         "zdotc": (32.0 * nc, lambda: rb.call("binnedBLAS_zbzdotc", FOLD, nc, x, 1, y, 1, zc)),
         "csum": (8.0 * (n // 2), lambda: rb.call("binnedBLAS_cbcsum", FOLD, n // 2, xf, 1, zcf)),
+        "dasum": (8.0 * n, lambda: rb.call("binnedBLAS_dbdasum", FOLD, n, x, 1, z)),
+        "sasum": (4.0 * n, lambda: rb.call("binnedBLAS_sbsasum", FOLD, n, xf, 1, zs)),
+        "dzasum": (16.0 * nc, lambda: rb.call("binnedBLAS_dbzasum", FOLD, nc, x, 1, z)),
+        "zdotu": (32.0 * nc, lambda: rb.call("binnedBLAS_zbzdotu", FOLD, nc, x, 1, y, 1, zc)),
+        "cdotc": (16.0 * (n // 2), lambda: rb.call("binnedBLAS_cbcdotc", FOLD, n // 2, xf, 1, yf, 1, zcf)),
     }
     out = {}
     for name, (byts, fn) in cases.items():

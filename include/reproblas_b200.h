@@ -95,6 +95,40 @@ void reproBLAS_rcsum_sub(const int fold, const int N, const void *X, const int i
                          void *sum);
 void reproBLAS_csum_sub(const int N, const void *X, const int incX, void *sum);
 
+/* include/reproBLAS.h:28 (src/reproBLAS/rdasum.c): sum of |x_i|; default fold:
+ * include/reproBLAS.h:98 */
+double reproBLAS_rdasum(const int fold, const int N, const double *X, const int incX);
+double reproBLAS_dasum(const int N, const double *X, const int incX);
+/* include/reproBLAS.h:33 (src/reproBLAS/rsasum.c); default fold: include/reproBLAS.h:103 */
+float reproBLAS_rsasum(const int fold, const int N, const float *X, const int incX);
+float reproBLAS_sasum(const int N, const float *X, const int incX);
+/* include/reproBLAS.h:38 (src/reproBLAS/rdzasum.c): sum of |re| + |im| of complex128;
+ * default fold: include/reproBLAS.h:108 */
+double reproBLAS_rdzasum(const int fold, const int N, const void *X, const int incX);
+double reproBLAS_dzasum(const int N, const void *X, const int incX);
+/* include/reproBLAS.h:44 (src/reproBLAS/rscasum.c): complex64; default fold:
+ * include/reproBLAS.h:114 */
+float reproBLAS_rscasum(const int fold, const int N, const void *X, const int incX);
+float reproBLAS_scasum(const int N, const void *X, const int incX);
+/* include/reproBLAS.h:41 (src/reproBLAS/rzdotu_sub.c): X^T Y into *dotu; default fold:
+ * include/reproBLAS.h:111 */
+void reproBLAS_rzdotu_sub(const int fold, const int N, const void *X, const int incX,
+                          const void *Y, const int incY, void *dotu);
+void reproBLAS_zdotu_sub(const int N, const void *X, const int incX, const void *Y,
+                         const int incY, void *dotu);
+/* include/reproBLAS.h:46-47 (src/reproBLAS/rcdotc_sub.c, rcdotu_sub.c): complex64 dots;
+ * default fold: include/reproBLAS.h:116-117. The result is the canonical binned state's
+ * value, which the reference returns whenever its 512-element blocks stay within the FP32
+ * endurance (always for calls of at most 256 elements). */
+void reproBLAS_rcdotc_sub(const int fold, const int N, const void *X, const int incX,
+                          const void *Y, const int incY, void *dotc);
+void reproBLAS_cdotc_sub(const int N, const void *X, const int incX, const void *Y,
+                         const int incY, void *dotc);
+void reproBLAS_rcdotu_sub(const int fold, const int N, const void *X, const int incX,
+                          const void *Y, const int incY, void *dotu);
+void reproBLAS_cdotu_sub(const int N, const void *X, const int incX, const void *Y,
+                         const int incY, void *dotu);
+
 /* include/reproBLAS.h:49 (src/reproBLAS/rdgemv.c:35-87):
  * y <- conv(binned(beta*y) + sum_j A_ij * fl(alpha*x_j)); Order 'r'/'R' row-major, else
  * column-major; TransA 'n'/'N' no transpose, else transpose. */
@@ -149,6 +183,28 @@ void binnedBLAS_zbzdotc(const int fold, const int N, const void *X, const int in
 /* include/binnedBLAS.h:76 (src/binnedBLAS/cbcsum.c -> cmcsum.ccog) */
 void binnedBLAS_cbcsum(const int fold, const int N, const void *X, const int incX,
                        float_complex_binned *Y);
+/* include/binnedBLAS.h:49 (src/binnedBLAS/dbdasum.c -> dmdasum.ccog:57-101) */
+void binnedBLAS_dbdasum(const int fold, const int N, const double *X, const int incX,
+                        double_binned *Y);
+/* include/binnedBLAS.h:69 (src/binnedBLAS/sbsasum.c -> smsasum.ccog) */
+void binnedBLAS_sbsasum(const int fold, const int N, const float *X, const int incX,
+                        float_binned *Y);
+/* include/binnedBLAS.h:58 (src/binnedBLAS/dbzasum.c -> dmzasum.ccog): |re| and |im| of
+ * complex128 into a real state */
+void binnedBLAS_dbzasum(const int fold, const int N, const void *X, const int incX,
+                        double_binned *Y);
+/* include/binnedBLAS.h:78 (src/binnedBLAS/sbcasum.c -> smcasum.ccog) */
+void binnedBLAS_sbcasum(const int fold, const int N, const void *X, const int incX,
+                        float_binned *Y);
+/* include/binnedBLAS.h:62 (src/binnedBLAS/zbzdotu.c -> zmzdotu.ccog:58-120) */
+void binnedBLAS_zbzdotu(const int fold, const int N, const void *X, const int incX,
+                        const void *Y, const int incY, double_complex_binned *Z);
+/* include/binnedBLAS.h:84, 82 (src/binnedBLAS/cbcdotc.c -> cmcdotc.ccog, cbcdotu.c ->
+ * cmcdotu.ccog); the canonical state, see reproBLAS_rcdotc_sub */
+void binnedBLAS_cbcdotc(const int fold, const int N, const void *X, const int incX,
+                        const void *Y, const int incY, float_complex_binned *Z);
+void binnedBLAS_cbcdotu(const int fold, const int N, const void *X, const int incX,
+                        const void *Y, const int incY, float_complex_binned *Z);
 
 /* include/binnedBLAS.h:87 (src/binnedBLAS/dbdgemv.ccog:57-162): Y (binned states, stride
  * incY states) += A*fl(alpha*x) or A^T*fl(alpha*x) */

@@ -51,6 +51,27 @@ SIGNATURES = {
     "binnedBLAS_zbzsum": (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp]),
     "binnedBLAS_zbzdotc": (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp, _c_int, _c_vp]),
     "binnedBLAS_cbcsum": (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp]),
+    "reproBLAS_rdasum": (_c_double, [_c_int, _c_int, _c_vp, _c_int]),
+    "reproBLAS_dasum": (_c_double, [_c_int, _c_vp, _c_int]),
+    "reproBLAS_rsasum": (_c_float, [_c_int, _c_int, _c_vp, _c_int]),
+    "reproBLAS_sasum": (_c_float, [_c_int, _c_vp, _c_int]),
+    "reproBLAS_rdzasum": (_c_double, [_c_int, _c_int, _c_vp, _c_int]),
+    "reproBLAS_dzasum": (_c_double, [_c_int, _c_vp, _c_int]),
+    "reproBLAS_rscasum": (_c_float, [_c_int, _c_int, _c_vp, _c_int]),
+    "reproBLAS_scasum": (_c_float, [_c_int, _c_vp, _c_int]),
+    "reproBLAS_rzdotu_sub": (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp, _c_int, _c_vp]),
+    "reproBLAS_zdotu_sub": (None, [_c_int, _c_vp, _c_int, _c_vp, _c_int, _c_vp]),
+    "reproBLAS_rcdotc_sub": (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp, _c_int, _c_vp]),
+    "reproBLAS_cdotc_sub": (None, [_c_int, _c_vp, _c_int, _c_vp, _c_int, _c_vp]),
+    "reproBLAS_rcdotu_sub": (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp, _c_int, _c_vp]),
+    "reproBLAS_cdotu_sub": (None, [_c_int, _c_vp, _c_int, _c_vp, _c_int, _c_vp]),
+    "binnedBLAS_dbdasum": (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp]),
+    "binnedBLAS_sbsasum": (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp]),
+    "binnedBLAS_dbzasum": (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp]),
+    "binnedBLAS_sbcasum": (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp]),
+    "binnedBLAS_zbzdotu": (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp, _c_int, _c_vp]),
+    "binnedBLAS_cbcdotc": (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp, _c_int, _c_vp]),
+    "binnedBLAS_cbcdotu": (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp, _c_int, _c_vp]),
     "reproBLAS_rdgemv": (None, [_c_int, _c_char, _c_char, _c_int, _c_int, _c_double, _c_vp,
                                 _c_int, _c_vp, _c_int, _c_double, _c_vp, _c_int]),
     "reproBLAS_dgemv": (None, [_c_char, _c_char, _c_int, _c_int, _c_double, _c_vp, _c_int,

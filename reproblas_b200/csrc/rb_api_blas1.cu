@@ -10,6 +10,7 @@
 //     the binned state is resumable, so chunking does not change a bit),
 //   * returns / copies out the converted result.
 #include <cmath>
+#include <climits>
 #include <cstring>
 #include <limits>
 
@@ -40,7 +41,7 @@ size_t elem_bytes(char t) { return t == 'd' ? 8 : t == 's' ? 4 : t == 'z' ? 16 :
 size_t real_bytes(char t) { return (t == 'd' || t == 'z') ? 8 : 4; }
 int comps(char t) { return (t == 'z' || t == 'c') ? 2 : 1; }
 bool is_dot(const Blas1Req& r) {
-  return comps(r.type) == 1 ? r.op == kOpDot : r.op == kOpCDotc;
+  return comps(r.type) == 1 ? r.op == kOpDot : (r.op == kOpCDotc || r.op == kOpCDotu);
 }
 
 cudaError_t launch(const Blas1Req& r, bool vec, int grid, int block, const Blas1Args& a,
@@ -247,6 +248,31 @@ double value_d(char type, int op, int fold, int N, const void* X, int incX, cons
   return run_blas1(r) ? out : qnan();
 }
 
+// Sum of |re| and |im| of a complex vector into one real state (dmzasum / smcasum): the
+// components taken as real values, contiguous when incX == 1, else the real parts and then
+// the imaginary parts (two strided passes into the same state; the state of a binned sum
+// does not depend on the order of its terms). `rt` is the component type ('d' or 's');
+// `acc` the caller's state or null, `result` the converted value or null.
+bool complex_asum(char rt, int fold, int N, const void* X, int incX, void* acc, void* result) {
+  const size_t cb = rt == 'd' ? 8 : 4;
+  if (N <= 0 || (incX == 1 && N <= INT_MAX / 2)) {
+    Blas1Req r{rt, kOpAsum, fold, N > 0 ? 2 * N : N, X, 1, nullptr, 0, acc, 0.0, nullptr, result,
+               false};
+    return run_blas1(r);
+  }
+  if (incX < 0 || incX > INT_MAX / 2) {
+    set_error(RB_ERR_INVALID_ARG, "negative or too large stride");
+    return false;
+  }
+  double tmp[2 * kMaxFold] = {};   // host state when the caller gave none (reals are 8 bytes)
+  float tmpf[2 * kMaxFold] = {};
+  void* st = acc ? acc : (rt == 'd' ? (void*)tmp : (void*)tmpf);
+  Blas1Req re{rt, kOpAsum, fold, N, X, 2 * incX, nullptr, 0, st, 0.0, nullptr, nullptr, false};
+  Blas1Req im{rt, kOpAsum, fold, N, (const unsigned char*)X + cb, 2 * incX, nullptr, 0, st, 0.0,
+              nullptr, result, false};
+  return run_blas1(re) && run_blas1(im);
+}
+
 }  // namespace
 }  // namespace rb
 
@@ -317,7 +343,96 @@ void reproBLAS_csum_sub(const int N, const void* X, const int incX, void* sum) {
   reproBLAS_rcsum_sub(3, N, X, incX, sum);
 }
 
+double reproBLAS_rdasum(const int fold, const int N, const double* X, const int incX) {
+  return rb::value_d('d', rb::kOpAsum, fold, N, X, incX, nullptr, 0, false);
+}
+double reproBLAS_dasum(const int N, const double* X, const int incX) {
+  return reproBLAS_rdasum(3, N, X, incX);
+}
+float reproBLAS_rsasum(const int fold, const int N, const float* X, const int incX) {
+  float out = 0.0f;
+  Blas1Req r{'s', rb::kOpAsum, fold, N, X, incX, nullptr, 0, nullptr, 0.0, nullptr, &out, false};
+  return rb::run_blas1(r) ? out : (float)rb::qnan();
+}
+float reproBLAS_sasum(const int N, const float* X, const int incX) {
+  return reproBLAS_rsasum(3, N, X, incX);
+}
+double reproBLAS_rdzasum(const int fold, const int N, const void* X, const int incX) {
+  double out = 0.0;
+  return rb::complex_asum('d', fold, N, X, incX, nullptr, &out) ? out : rb::qnan();
+}
+double reproBLAS_dzasum(const int N, const void* X, const int incX) {
+  return reproBLAS_rdzasum(3, N, X, incX);
+}
+float reproBLAS_rscasum(const int fold, const int N, const void* X, const int incX) {
+  float out = 0.0f;
+  return rb::complex_asum('s', fold, N, X, incX, nullptr, &out) ? out : (float)rb::qnan();
+}
+float reproBLAS_scasum(const int N, const void* X, const int incX) {
+  return reproBLAS_rscasum(3, N, X, incX);
+}
+void reproBLAS_rzdotu_sub(const int fold, const int N, const void* X, const int incX,
+                          const void* Y, const int incY, void* dotu) {
+  Blas1Req r{'z', rb::kOpCDotu, fold, N, X, incX, Y, incY, nullptr, 0.0, nullptr, dotu, false};
+  rb::run_blas1(r);
+}
+void reproBLAS_zdotu_sub(const int N, const void* X, const int incX, const void* Y,
+                         const int incY, void* dotu) {
+  reproBLAS_rzdotu_sub(3, N, X, incX, Y, incY, dotu);
+}
+void reproBLAS_rcdotc_sub(const int fold, const int N, const void* X, const int incX,
+                          const void* Y, const int incY, void* dotc) {
+  Blas1Req r{'c', rb::kOpCDotc, fold, N, X, incX, Y, incY, nullptr, 0.0, nullptr, dotc, false};
+  rb::run_blas1(r);
+}
+void reproBLAS_cdotc_sub(const int N, const void* X, const int incX, const void* Y,
+                         const int incY, void* dotc) {
+  reproBLAS_rcdotc_sub(3, N, X, incX, Y, incY, dotc);
+}
+void reproBLAS_rcdotu_sub(const int fold, const int N, const void* X, const int incX,
+                          const void* Y, const int incY, void* dotu) {
+  Blas1Req r{'c', rb::kOpCDotu, fold, N, X, incX, Y, incY, nullptr, 0.0, nullptr, dotu, false};
+  rb::run_blas1(r);
+}
+void reproBLAS_cdotu_sub(const int N, const void* X, const int incX, const void* Y,
+                         const int incY, void* dotu) {
+  reproBLAS_rcdotu_sub(3, N, X, incX, Y, incY, dotu);
+}
+
 // ---- binnedBLAS level ------------------------------------------------------------------------
+void binnedBLAS_dbdasum(const int fold, const int N, const double* X, const int incX,
+                        double_binned* Y) {
+  Blas1Req r{'d', rb::kOpAsum, fold, N, X, incX, nullptr, 0, Y, 0.0, nullptr, nullptr, false};
+  rb::run_blas1(r);
+}
+void binnedBLAS_sbsasum(const int fold, const int N, const float* X, const int incX,
+                        float_binned* Y) {
+  Blas1Req r{'s', rb::kOpAsum, fold, N, X, incX, nullptr, 0, Y, 0.0, nullptr, nullptr, false};
+  rb::run_blas1(r);
+}
+void binnedBLAS_dbzasum(const int fold, const int N, const void* X, const int incX,
+                        double_binned* Y) {
+  rb::complex_asum('d', fold, N, X, incX, Y, nullptr);
+}
+void binnedBLAS_sbcasum(const int fold, const int N, const void* X, const int incX,
+                        float_binned* Y) {
+  rb::complex_asum('s', fold, N, X, incX, Y, nullptr);
+}
+void binnedBLAS_zbzdotu(const int fold, const int N, const void* X, const int incX,
+                        const void* Y, const int incY, double_complex_binned* Z) {
+  Blas1Req r{'z', rb::kOpCDotu, fold, N, X, incX, Y, incY, Z, 0.0, nullptr, nullptr, false};
+  rb::run_blas1(r);
+}
+void binnedBLAS_cbcdotc(const int fold, const int N, const void* X, const int incX,
+                        const void* Y, const int incY, float_complex_binned* Z) {
+  Blas1Req r{'c', rb::kOpCDotc, fold, N, X, incX, Y, incY, Z, 0.0, nullptr, nullptr, false};
+  rb::run_blas1(r);
+}
+void binnedBLAS_cbcdotu(const int fold, const int N, const void* X, const int incX,
+                        const void* Y, const int incY, float_complex_binned* Z) {
+  Blas1Req r{'c', rb::kOpCDotu, fold, N, X, incX, Y, incY, Z, 0.0, nullptr, nullptr, false};
+  rb::run_blas1(r);
+}
 void binnedBLAS_dbdsum(const int fold, const int N, const double* X, const int incX,
                        double_binned* Y) {
   Blas1Req r{'d', rb::kOpSum, fold, N, X, incX, nullptr, 0, Y, 0.0, nullptr, nullptr, false};

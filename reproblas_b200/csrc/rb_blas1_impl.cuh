@@ -118,6 +118,12 @@ struct Red1 {
   __device__ __forceinline__ void tile(const T (&x)[K], const T (&y)[K], int nv) {
     if (OP == kOpSum) {
       a.template tile<K>(x, nv);
+    } else if (OP == kOpAsum) {
+      // depositASum.py: the absolute values (NaN stays NaN, either infinity becomes +Inf)
+      T v[K];
+#pragma unroll
+      for (int k = 0; k < K; k++) v[k] = BT<T>::from(BT<T>::bits(x[k]) & BT<T>::kAbsMask);
+      a.template tile<K>(v, nv);
     } else if (OP == kOpDot) {
       T v[K];
 #pragma unroll
@@ -416,6 +422,24 @@ template <> struct Pair<float> {
   static __device__ __forceinline__ V ld(const float* p) { return __ldg((const float2*)p); }
 };
 
+// The four products of one complex element, each deposited separately: the real part
+// receives r0 and r1, the imaginary part i0 and i1.
+//   conj(x)*y: xr*yr, xi*yi | xr*yi, -(xi*yr)   (depositDotC.py:14-23)
+//   x*y:       xr*yr, -(xi*yi) | xr*yi, xi*yr   (depositDotU.py:14-24)
+template <int OP, typename T>
+__device__ __forceinline__ void cprod(T xr, T xi, T yr, T yi, T& r0, T& r1, T& i0, T& i1) {
+  using B = BT<T>;
+  r0 = B::mul(xr, yr);
+  i0 = B::mul(xr, yi);
+  if (OP == kOpCDotc) {
+    r1 = B::mul(xi, yi);
+    i1 = -B::mul(xi, yr);
+  } else {
+    r1 = -B::mul(xi, yi);
+    i1 = B::mul(xi, yr);
+  }
+}
+
 // Three CTAs per SM for double complex (80 registers), four for float complex.
 // VEC: the body [head, body_end) is read in warp tiles of 16-byte vectors (contiguous,
 // aligned inputs; the host plans head and body_end with blas1_complex_tile()); everything
@@ -470,10 +494,8 @@ blasc_kernel(Blas1Args args) {
 #pragma unroll
           for (int j = 0; j < VW; j++) {
             const int e = k * VW + j;
-            vr[2 * e] = B::mul(xr[e], t[2 * j]);
-            vr[2 * e + 1] = B::mul(xi[e], t[2 * j + 1]);
-            vi[2 * e] = B::mul(xr[e], t[2 * j + 1]);
-            vi[2 * e + 1] = -B::mul(xi[e], t[2 * j]);
+            cprod<OP>(xr[e], xi[e], t[2 * j], t[2 * j + 1], vr[2 * e], vr[2 * e + 1],
+                      vi[2 * e], vi[2 * e + 1]);
           }
         }
         tile2<T, F, 2 * E>(st.re, vr, st.im, vi);
@@ -504,8 +526,7 @@ blasc_kernel(Blas1Args args) {
       if (nv == K) tile2<T, F, K>(st.re, vr, st.im, vi);
       else { st.re.template tile<K>(vr, nv); st.im.template tile<K>(vi, nv); }
     } else {
-      // conj(x)*y: real part receives xr*yr and xi*yi, imaginary part xr*yi and
-      // -(xi*yr), each product deposited separately (depositDotC.py:14-23)
+      // products deposited separately, see cprod
       T vr[2 * K], vi[2 * K];
       int nv = 0;
 #pragma unroll
@@ -516,10 +537,7 @@ blasc_kernel(Blas1Args args) {
           const long long e = i < head ? i : body_end + (i - head);
           auto xv = Pair<T>::ld(x + 2 * e * args.incx);
           auto yv = Pair<T>::ld(y + 2 * e * args.incy);
-          vr[2 * k] = B::mul(xv.x, yv.x);
-          vr[2 * k + 1] = B::mul(xv.y, yv.y);
-          vi[2 * k] = B::mul(xv.x, yv.y);
-          vi[2 * k + 1] = -B::mul(xv.y, yv.x);
+          cprod<OP>(xv.x, xv.y, yv.x, yv.y, vr[2 * k], vr[2 * k + 1], vi[2 * k], vi[2 * k + 1]);
           nv = 2 * k + 2;
         }
       }
@@ -622,6 +640,9 @@ cudaError_t launch_real(int op, bool vec, int grid, int block, const Blas1Args& 
   } else if (op == kOpSsq && sizeof(T) == 8) {
     if (vec) blas1_kernel<T, F, kOpSsq, true><<<grid, block, 0, s>>>(a);
     else blas1_kernel<T, F, kOpSsq, false><<<grid, block, 0, s>>>(a);
+  } else if (op == kOpAsum) {
+    if (vec) blas1_kernel<T, F, kOpAsum, true><<<grid, block, 0, s>>>(a);
+    else blas1_kernel<T, F, kOpAsum, false><<<grid, block, 0, s>>>(a);
   } else {
     return cudaErrorInvalidValue;
   }
@@ -633,9 +654,12 @@ cudaError_t launch_cplx(int op, bool vec, int grid, int block, const Blas1Args& 
   if (op == kOpCSum) {
     if (vec) blasc_kernel<T, F, kOpCSum, true><<<grid, block, 0, s>>>(a);
     else blasc_kernel<T, F, kOpCSum, false><<<grid, block, 0, s>>>(a);
-  } else if (op == kOpCDotc && sizeof(T) == 8) {
+  } else if (op == kOpCDotc) {
     if (vec) blasc_kernel<T, F, kOpCDotc, true><<<grid, block, 0, s>>>(a);
     else blasc_kernel<T, F, kOpCDotc, false><<<grid, block, 0, s>>>(a);
+  } else if (op == kOpCDotu) {
+    if (vec) blasc_kernel<T, F, kOpCDotu, true><<<grid, block, 0, s>>>(a);
+    else blasc_kernel<T, F, kOpCDotu, false><<<grid, block, 0, s>>>(a);
   } else {
     return cudaErrorInvalidValue;
   }
@@ -652,8 +676,16 @@ template <typename T, int F>
 const void* real_kernel_ptr(int op, bool vec) {
   if (op == kOpSum) return vec ? (const void*)blas1_kernel<T, F, kOpSum, true> : (const void*)blas1_kernel<T, F, kOpSum, false>;
   if (op == kOpDot) return vec ? (const void*)blas1_kernel<T, F, kOpDot, true> : (const void*)blas1_kernel<T, F, kOpDot, false>;
+  if (op == kOpAsum) return vec ? (const void*)blas1_kernel<T, F, kOpAsum, true> : (const void*)blas1_kernel<T, F, kOpAsum, false>;
   if (sizeof(T) == 8) return vec ? (const void*)blas1_kernel<T, F, kOpSsq, true> : (const void*)blas1_kernel<T, F, kOpSsq, false>;
   return nullptr;
+}
+
+template <typename T, int F>
+const void* cplx_kernel_ptr(int op, bool vec) {
+  if (op == kOpCSum) return vec ? (const void*)blasc_kernel<T, F, kOpCSum, true> : (const void*)blasc_kernel<T, F, kOpCSum, false>;
+  if (op == kOpCDotc) return vec ? (const void*)blasc_kernel<T, F, kOpCDotc, true> : (const void*)blasc_kernel<T, F, kOpCDotc, false>;
+  return vec ? (const void*)blasc_kernel<T, F, kOpCDotu, true> : (const void*)blasc_kernel<T, F, kOpCDotu, false>;
 }
 
 template <int F>
@@ -661,11 +693,8 @@ const void* blas1_kernel_ptr(char type, int op, bool vec) {
   switch (type) {
     case 'd': return real_kernel_ptr<double, F>(op, vec);
     case 's': return real_kernel_ptr<float, F>(op, vec);
-    case 'z':
-      if (op == kOpCSum) return vec ? (const void*)blasc_kernel<double, F, kOpCSum, true> : (const void*)blasc_kernel<double, F, kOpCSum, false>;
-      return vec ? (const void*)blasc_kernel<double, F, kOpCDotc, true> : (const void*)blasc_kernel<double, F, kOpCDotc, false>;
-    default:
-      return vec ? (const void*)blasc_kernel<float, F, kOpCSum, true> : (const void*)blasc_kernel<float, F, kOpCSum, false>;
+    case 'z': return cplx_kernel_ptr<double, F>(op, vec);
+    default: return cplx_kernel_ptr<float, F>(op, vec);
   }
 }
 

@@ -12,11 +12,13 @@ enum Op1 : int {
   kOpSum = 0,   // sum x_i                       (dmdsum / smssum)
   kOpDot = 1,   // sum fl(x_i * y_i)             (dmddot / smsdot)
   kOpSsq = 2,   // sum fl((x_i * (1/scl))^2)     (dmdssq), running power-of-two scale
+  kOpAsum = 3,  // sum |x_i|                     (dmdasum / smsasum)
 };
 // Complex BLAS1 reductions (two accumulators, real and imaginary)
 enum OpC : int {
   kOpCSum = 0,   // sum x_i                      (zmzsum / cmcsum)
-  kOpCDotc = 1,  // sum conj(x_i) * y_i          (zmzdotc)
+  kOpCDotc = 1,  // sum conj(x_i) * y_i          (zmzdotc / cmcdotc)
+  kOpCDotu = 2,  // sum x_i * y_i                (zmzdotu / cmcdotu)
 };
 
 // Workspace used by a grid-wide reduction: one partial record per CTA plus an arrival
