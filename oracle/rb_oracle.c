@@ -1004,6 +1004,239 @@ void rbo_cbcdotu(int fold, int N, const void *X, int incX, const void *Y, int in
 }
 
 /* ------------------------------------------------------------------------- */
+/* Scaled sums of squares: FP32, complex128, complex64                          */
+/* ------------------------------------------------------------------------- */
+#define NB_SSSQ 512     /* src/binnedBLAS/smsssq.ccog:36 */
+#define NB_ZSSQ 1024    /* src/binnedBLAS/dmzssq.ccog:36 */
+#define NB_CSSQ 256     /* src/binnedBLAS/smcssq.ccog:36 */
+
+/* src/binned/sscale.c */
+float rbo_sscale(float x) {
+  int e = fexp(x);
+  e = e < SBW ? SBW : e;
+  e -= (e - SEXP_BIAS - 1) % SBW;
+  e -= SEXP_BIAS;
+  return ldexpf(0.5f, e);
+}
+
+/* src/binned/smsrescale.c */
+static void smsrescale(int fold, float x, float scaleY, float *pri, int incpri, float *car,
+                       int inccar) {
+  if (x == scaleY || x == 0.0f || scaleY == 0.0f) return;
+  float r = x / scaleY;
+  r *= r;
+  for (int i = 0; i < fold; i++) {
+    pri[i * incpri] /= r;
+    if (pri[i * incpri] == 0.0f) {
+      rbo_smsupdate(fold - i, 0.0f, pri + i * incpri, incpri, car + i * inccar, inccar);
+      return;
+    }
+  }
+}
+
+/* src/binned/smsmaddsq.c */
+static float smsmaddsq(int fold, float scaleX, const float *priX, int incpriX, const float *carX,
+                       int inccarX, float scaleY, float *priY, int incpriY, float *carY,
+                       int inccarY) {
+  if (scaleX > scaleY) {
+    smsrescale(fold, scaleX, scaleY, priY, incpriY, carY, inccarY);
+    rbo_smsmadd(fold, priX, incpriX, carX, inccarX, priY, incpriY, carY, inccarY);
+    return scaleX;
+  } else if (scaleX == scaleY) {
+    rbo_smsmadd(fold, priX, incpriX, carX, inccarX, priY, incpriY, carY, inccarY);
+    return scaleX;
+  } else {
+    float tmp[2 * SMAXFOLD];
+    for (int i = 0; i < fold; i++) { tmp[i] = priX[i * incpriX]; tmp[fold + i] = carX[i * inccarX]; }
+    smsrescale(fold, scaleY, scaleX, tmp, 1, tmp + fold, 1);
+    rbo_smsmadd(fold, tmp, 1, tmp + fold, 1, priY, incpriY, carY, inccarY);
+    return scaleY;
+  }
+}
+
+/* src/binned/dmdmaddsq.c on manually strided states */
+static double dmdmaddsq(int fold, double scaleX, const double *priX, int incpriX,
+                        const double *carX, int inccarX, double scaleY, double *priY,
+                        int incpriY, double *carY, int inccarY) {
+  if (scaleX > scaleY) {
+    rbo_dmdrescale(fold, scaleX, scaleY, priY, incpriY, carY, inccarY);
+    rbo_dmdmadd(fold, priX, incpriX, carX, inccarX, priY, incpriY, carY, inccarY);
+    return scaleX;
+  } else if (scaleX == scaleY) {
+    rbo_dmdmadd(fold, priX, incpriX, carX, inccarX, priY, incpriY, carY, inccarY);
+    return scaleX;
+  } else {
+    double tmp[2 * DMAXFOLD];
+    for (int i = 0; i < fold; i++) { tmp[i] = priX[i * incpriX]; tmp[fold + i] = carX[i * inccarX]; }
+    rbo_dmdrescale(fold, scaleY, scaleX, tmp, 1, tmp + fold, 1);
+    rbo_dmdmadd(fold, tmp, 1, tmp + fold, 1, priY, incpriY, carY, inccarY);
+    return scaleY;
+  }
+}
+
+/* src/binned/zmdrescale.c and cmsrescale.c, as written: both components are divided, and
+ * the zero test looks at element i * incpri of the interleaved primaries. */
+static void zmdrescale(int fold, double x, double scaleY, double *pri, int incpri, double *car,
+                       int inccar) {
+  if (x == scaleY || x == 0.0 || scaleY == 0.0) return;
+  double r = x / scaleY;
+  r *= r;
+  for (int i = 0; i < fold; i++) {
+    pri[i * 2 * incpri] /= r;
+    pri[i * 2 * incpri + 1] /= r;
+    if (pri[i * incpri] == 0.0) {
+      rbo_dmdupdate(fold - i, 0.0, pri + i * 2 * incpri, 2 * incpri, car + i * 2 * inccar, 2 * inccar);
+      rbo_dmdupdate(fold - i, 0.0, pri + i * 2 * incpri + 1, 2 * incpri, car + i * 2 * inccar + 1,
+                    2 * inccar);
+      break;
+    }
+  }
+}
+
+static void cmsrescale(int fold, float x, float scaleY, float *pri, int incpri, float *car,
+                       int inccar) {
+  if (x == scaleY || x == 0.0f || scaleY == 0.0f) return;
+  float r = x / scaleY;
+  r *= r;
+  for (int i = 0; i < fold; i++) {
+    pri[i * 2 * incpri] /= r;
+    pri[i * 2 * incpri + 1] /= r;
+    if (pri[i * incpri] == 0.0f) {
+      rbo_smsupdate(fold - i, 0.0f, pri + i * 2 * incpri, 2 * incpri, car + i * 2 * inccar, 2 * inccar);
+      rbo_smsupdate(fold - i, 0.0f, pri + i * 2 * incpri + 1, 2 * incpri, car + i * 2 * inccar + 1,
+                    2 * inccar);
+      return;
+    }
+  }
+}
+
+/* src/binnedBLAS/smsssq.ccog (via sbsssq.c): float scale, squares of x * (1/scale) */
+float rbo_sbsssq(int fold, int N, const float *X, int incX, float scaleY, float *Y) {
+  float *pri = Y, *car = Y + fold;
+  float scl = scaleY;
+  int deposits = 0;
+  for (int i = 0; i < N; i += NB_SSSQ) {
+    int nb = imin(N - i, NB_SSSQ);
+    const float *x = X + (size_t)i * incX;
+    float amax = 0.0f;
+    for (int j = 0; j < nb; j++) amax = smaxabs(amax, x[(size_t)j * incX]);
+    if (isinf(amax) || isinf(pri[0]))
+      for (int j = 0; j < nb; j++) pri[0] += fabsf(x[(size_t)j * incX]);
+    if (isnan(pri[0])) return rbo_sscale(1.0f);
+    if (isinf(pri[0])) continue;
+    if (deposits + nb > SENDURANCE) { rbo_smrenorm(fold, pri, 1, car, 1); deposits = 0; }
+    float nscl = rbo_sscale(amax);
+    if (nscl > scl) {
+      if (scl > 0.0f) smsrescale(fold, nscl, scl, pri, 1, car, 1);
+      scl = nscl;
+    }
+    amax /= scl;
+    amax = amax * amax;
+    rbo_smsupdate(fold, amax, pri, 1, car, 1);
+    float inv = (float)(1.0 / scl);
+    for (int j = 0; j < nb; j++) {
+      float v = x[(size_t)j * incX] * inv;
+      rbo_smsdeposit(fold, v * v, pri, 1);
+    }
+    deposits += nb;
+  }
+  rbo_smrenorm(fold, pri, 1, car, 1);
+  return fnonfinite(pri[0]) ? rbo_sscale(1.0f) : scl;
+}
+
+/* src/binnedBLAS/dmzssq.ccog (via dbzssq.c): the squares of the two components go to a
+ * temporary complex state (scale starting at 0, components sharing one index), merged into
+ * Y at the end with dmdmaddsq, real part first. */
+double rbo_dbzssq(int fold, int N, const void *Xv, int incX, double scaleY, double *Y) {
+  const double *X = (const double *)Xv;
+  double t[4 * DMAXFOLD] = {0};
+  double scl = 0.0;
+  int deposits = 0;
+  for (int i = 0; i < N; i += NB_ZSSQ) {
+    int nb = imin(N - i, NB_ZSSQ);
+    const double *x = X + 2 * (size_t)i * incX;
+    double amax = 0.0;
+    for (int j = 0; j < nb; j++) {
+      amax = dmaxabs(amax, x[2 * (size_t)j * incX]);
+      amax = dmaxabs(amax, x[2 * (size_t)j * incX + 1]);
+    }
+    if (isinf(amax) || isinf(Y[0]))
+      for (int j = 0; j < nb; j++) {
+        Y[0] += fabs(x[2 * (size_t)j * incX]);
+        Y[0] += fabs(x[2 * (size_t)j * incX + 1]);
+      }
+    if (isnan(Y[0]) || isnan(t[0]) || isnan(t[1])) { Y[0] += t[0] + t[1]; return rbo_dscale(1.0); }
+    if (isinf(Y[0])) continue;
+    if (deposits + nb > DENDURANCE) { zrenorm(fold, t); deposits = 0; }
+    double nscl = rbo_dscale(amax);
+    if (nscl > scl) {
+      if (scl > 0.0) zmdrescale(fold, nscl, scl, t, 1, t + 2 * fold, 1);
+      scl = nscl;
+    }
+    amax /= scl;
+    amax = amax * amax;
+    rbo_dmdupdate(fold, amax, t, 2, t + 2 * fold, 2);
+    rbo_dmdupdate(fold, amax, t + 1, 2, t + 2 * fold + 1, 2);
+    double inv = 1.0 / scl;
+    for (int j = 0; j < nb; j++) {
+      double vr = x[2 * (size_t)j * incX] * inv, vi = x[2 * (size_t)j * incX + 1] * inv;
+      zdeposit_component(fold, vr * vr, t);
+      zdeposit_component(fold, vi * vi, t + 1);
+    }
+    deposits += nb;
+  }
+  zrenorm(fold, t);
+  double s1 = dmdmaddsq(fold, scl, t, 2, t + 2 * fold, 2, scaleY, Y, 1, Y + fold, 1);
+  scl = dmdmaddsq(fold, scl, t + 1, 2, t + 2 * fold + 1, 2, s1, Y, 1, Y + fold, 1);
+  return dnonfinite(Y[0]) ? rbo_dscale(1.0) : scl;
+}
+
+/* src/binnedBLAS/smcssq.ccog (via sbcssq.c): the float form of dmzssq */
+float rbo_sbcssq(int fold, int N, const void *Xv, int incX, float scaleY, float *Y) {
+  const float *X = (const float *)Xv;
+  float t[4 * SMAXFOLD] = {0};
+  float scl = 0.0f;
+  int deposits = 0;
+  for (int i = 0; i < N; i += NB_CSSQ) {
+    int nb = imin(N - i, NB_CSSQ);
+    const float *x = X + 2 * (size_t)i * incX;
+    float amax = 0.0f;
+    for (int j = 0; j < nb; j++) {
+      amax = smaxabs(amax, x[2 * (size_t)j * incX]);
+      amax = smaxabs(amax, x[2 * (size_t)j * incX + 1]);
+    }
+    if (isinf(amax) || isinf(Y[0]))
+      for (int j = 0; j < nb; j++) {
+        Y[0] += fabsf(x[2 * (size_t)j * incX]);
+        Y[0] += fabsf(x[2 * (size_t)j * incX + 1]);
+      }
+    if (isnan(Y[0]) || isnan(t[0]) || isnan(t[1])) { Y[0] += t[0] + t[1]; return rbo_sscale(1.0f); }
+    if (isinf(Y[0])) continue;
+    if (deposits + nb > SENDURANCE) { crenorm(fold, t); deposits = 0; }
+    float nscl = rbo_sscale(amax);
+    if (nscl > scl) {
+      if (scl > 0.0f) cmsrescale(fold, nscl, scl, t, 1, t + 2 * fold, 1);
+      scl = nscl;
+    }
+    amax /= scl;
+    amax = amax * amax;
+    rbo_smsupdate(fold, amax, t, 2, t + 2 * fold, 2);
+    rbo_smsupdate(fold, amax, t + 1, 2, t + 2 * fold + 1, 2);
+    float inv = (float)(1.0 / scl);
+    for (int j = 0; j < nb; j++) {
+      float vr = x[2 * (size_t)j * incX] * inv, vi = x[2 * (size_t)j * incX + 1] * inv;
+      cdeposit_component(fold, vr * vr, t);
+      cdeposit_component(fold, vi * vi, t + 1);
+    }
+    deposits += nb;
+  }
+  crenorm(fold, t);
+  float s1 = smsmaddsq(fold, scl, t, 2, t + 2 * fold, 2, scaleY, Y, 1, Y + fold, 1);
+  scl = smsmaddsq(fold, scl, t + 1, 2, t + 2 * fold + 1, 2, s1, Y, 1, Y + fold, 1);
+  return fnonfinite(Y[0]) ? rbo_sscale(1.0f) : scl;
+}
+
+/* ------------------------------------------------------------------------- */
 /* BLAS2/3: src/binnedBLAS/dbdgemv.ccog:57-162, dbdgemm.ccog:61-420            */
 /* ------------------------------------------------------------------------- */
 static int is_row_major(char o) { return o == 'r' || o == 'R'; }
@@ -1176,6 +1409,24 @@ void rbo_rcdotu_sub(int fold, int N, const void *X, int incX, const void *Y, int
   float acc[4 * SMAXFOLD] = {0};
   rbo_cbcdotu(fold, N, X, incX, Y, incY, acc);
   cconv(fold, acc, (float *)dotu);
+}
+
+float rbo_rsnrm2(int fold, int N, const float *X, int incX) {       /* rsnrm2.c */
+  float acc[2 * SMAXFOLD] = {0};
+  float scl = rbo_sbsssq(fold, N, X, incX, 0.0f, acc);
+  return (float)(scl * sqrt(rbo_ssbconv(fold, acc)));
+}
+
+double rbo_rdznrm2(int fold, int N, const void *X, int incX) {      /* rdznrm2.c */
+  double acc[2 * DMAXFOLD] = {0};
+  double scl = rbo_dbzssq(fold, N, X, incX, 0.0, acc);
+  return scl * sqrt(rbo_ddbconv(fold, acc));
+}
+
+float rbo_rscnrm2(int fold, int N, const void *X, int incX) {       /* rscnrm2.c */
+  float acc[2 * SMAXFOLD] = {0};
+  float scl = rbo_sbcssq(fold, N, X, incX, 0.0f, acc);
+  return (float)(scl * sqrt(rbo_ssbconv(fold, acc)));
 }
 
 /* rdgemv.c:35-87: y <- conv(binned(beta*y) + sum_j A_ij*(alpha*x_j)) */

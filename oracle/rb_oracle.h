@@ -71,6 +71,10 @@ void   rbo_sbcasum(int fold, int N, const void *X, int incX, float *Y);
 void   rbo_zbzdotu(int fold, int N, const void *X, int incX, const void *Y, int incY, double *Z);
 void   rbo_cbcdotc(int fold, int N, const void *X, int incX, const void *Y, int incY, float *Z);
 void   rbo_cbcdotu(int fold, int N, const void *X, int incX, const void *Y, int incY, float *Z);
+float  rbo_sscale(float x);
+float  rbo_sbsssq(int fold, int N, const float *X, int incX, float scaleY, float *Y);
+double rbo_dbzssq(int fold, int N, const void *X, int incX, double scaleY, double *Y);
+float  rbo_sbcssq(int fold, int N, const void *X, int incX, float scaleY, float *Y);
 void   rbo_dbdgemv(int fold, char Order, char TransA, int M, int N, double alpha,
                    const double *A, int lda, const double *X, int incX, double *Y, int incY);
 void   rbo_dbdgemm(int fold, char Order, char TransA, char TransB, int M, int N, int K,
@@ -93,6 +97,9 @@ float  rbo_rscasum(int fold, int N, const void *X, int incX);
 void   rbo_rzdotu_sub(int fold, int N, const void *X, int incX, const void *Y, int incY, void *dotu);
 void   rbo_rcdotc_sub(int fold, int N, const void *X, int incX, const void *Y, int incY, void *dotc);
 void   rbo_rcdotu_sub(int fold, int N, const void *X, int incX, const void *Y, int incY, void *dotu);
+float  rbo_rsnrm2(int fold, int N, const float *X, int incX);
+double rbo_rdznrm2(int fold, int N, const void *X, int incX);
+float  rbo_rscnrm2(int fold, int N, const void *X, int incX);
 void   rbo_rdgemv(int fold, char Order, char TransA, int M, int N, double alpha,
                   const double *A, int lda, const double *X, int incX,
                   double beta, double *Y, int incY);

@@ -37,6 +37,12 @@ _SIGS = {
     "zbzdotu": (None, [c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp]),
     "cbcdotc": (None, [c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp]),
     "cbcdotu": (None, [c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp]),
+    "sbsssq": (c_float, [c_int, c_int, c_vp, c_int, c_float, c_vp]),
+    "dbzssq": (c_double, [c_int, c_int, c_vp, c_int, c_double, c_vp]),
+    "sbcssq": (c_float, [c_int, c_int, c_vp, c_int, c_float, c_vp]),
+    "rsnrm2": (c_float, [c_int, c_int, c_vp, c_int]),
+    "rdznrm2": (c_double, [c_int, c_int, c_vp, c_int]),
+    "rscnrm2": (c_float, [c_int, c_int, c_vp, c_int]),
     "rdasum": (c_double, [c_int, c_int, c_vp, c_int]),
     "rsasum": (c_float, [c_int, c_int, c_vp, c_int]),
     "rdzasum": (c_double, [c_int, c_int, c_vp, c_int]),
@@ -89,6 +95,8 @@ _REF_NAMES = {
     "rdzasum": "reproBLAS_rdzasum", "rscasum": "reproBLAS_rscasum",
     "rzdotu_sub": "reproBLAS_rzdotu_sub", "rcdotc_sub": "reproBLAS_rcdotc_sub",
     "rcdotu_sub": "reproBLAS_rcdotu_sub",
+    "sbsssq": "binnedBLAS_sbsssq", "dbzssq": "binnedBLAS_dbzssq", "sbcssq": "binnedBLAS_sbcssq",
+    "rsnrm2": "reproBLAS_rsnrm2", "rdznrm2": "reproBLAS_rdznrm2", "rscnrm2": "reproBLAS_rscnrm2",
     "dbdbadd": "binned_dbdbadd", "dbdconv": "binned_dbdconv", "ddbconv": "binned_ddbconv",
     "dbdbaddsq": "binned_dbdbaddsq", "dbbound": "binned_dbbound", "dscale": "binned_dscale",
     "dindex": "binned_dindex", "sindex": "binned_sindex", "sbsbadd": "binned_sbsbadd",

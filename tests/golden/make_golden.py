@@ -117,6 +117,15 @@ def main():
                     z = ref_chunked(fn, fold, n, xc, yc)
                     c[nm] = hexb(z)
                     c["r" + nm[3:]] = hexb(cconv(R, fold, z))
+                z = binned_zeros(fold, "s"); sc = R.sbsssq(fold, n, ptr(xf), 1, 0.0, ptr(z))
+                c["sbsssq"] = hexb(z); c["sbsssq_scale"] = hexb(np.float32(sc))
+                z = binned_zeros(fold); sc = R.dbzssq(fold, n, ptr(xz), 1, 0.0, ptr(z))
+                c["dbzssq"] = hexb(z); c["dbzssq_scale"] = hexb(np.float64(sc))
+                z = binned_zeros(fold, "s"); sc = R.sbcssq(fold, n, ptr(xc), 1, 0.0, ptr(z))
+                c["sbcssq"] = hexb(z); c["sbcssq_scale"] = hexb(np.float32(sc))
+                c["rsnrm2"] = hexb(np.float32(R.rsnrm2(fold, n, ptr(xf), 1)))
+                c["rdznrm2"] = hexb(np.float64(R.rdznrm2(fold, n, ptr(xz), 1)))
+                c["rscnrm2"] = hexb(np.float32(R.rscnrm2(fold, n, ptr(xc), 1)))
                 more.append(c)
 
     # The dsum configuration quoted by the benchmark: N = 2^20, fold 3, sine and uniform

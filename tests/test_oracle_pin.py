@@ -298,3 +298,54 @@ def test_port_matches_golden_asum_dots(port, golden):
             if not same_value(o, from_hex(c[name], dt)):
                 bad.append((name, key))
     assert not bad, bad[:10]
+
+
+def test_port_matches_golden_ssq_more(port, golden):
+    bad = []
+    for c in golden["blas1_more"]:
+        dist, n, fold = c["dist"], c["n"], c["fold"]
+        xf = gen(dist, n, 11, np.float32)
+        xz, xc = gen_complex(dist, n, 11), gen_complex(dist, n, 11, np.complex64)
+        key = (dist, n, fold)
+        for name, kind, x, dt in [("sbsssq", "s", xf, np.float32), ("dbzssq", "d", xz, np.float64),
+                                  ("sbcssq", "s", xc, np.float32)]:
+            z = binned_zeros(fold, kind)
+            sc = getattr(port, name)(fold, n, ptr(x), 1, 0.0, ptr(z))
+            if not same_state(z, from_hex(c[name], dt), fold):
+                bad.append((name, key))
+            if not same_value(np.asarray(sc, dt), from_hex(c[name + "_scale"], dt)[0]):
+                bad.append((name + "_scale", key))
+        for name, x, dt in [("rsnrm2", xf, np.float32), ("rdznrm2", xz, np.float64),
+                            ("rscnrm2", xc, np.float32)]:
+            if not same_value(np.asarray(getattr(port, name)(fold, n, ptr(x), 1), dt),
+                              from_hex(c[name], dt)[0]):
+                bad.append((name, key))
+    assert not bad, bad[:10]
+
+
+@needs_ref
+@pytest.mark.parametrize("inc", [1, 2])
+def test_port_matches_reference_live_ssq_more(port, inc):
+    """FP32 and complex scaled sums of squares, accumulated into scaled non-empty states."""
+    R = ref()
+    rng = np.random.default_rng(321)
+    for trial in range(30):
+        n = int(rng.integers(0, 5000))
+        fold = int(rng.integers(2, 9))
+        dist = ["uniform", "normal", "loguniform", "illcond", "huge", "tiny"][trial % 6]
+        xf = gen(dist, n * inc + 1, trial, np.float32)
+        xz = gen_complex(dist, n * inc + 1, trial)
+        xc = gen_complex(dist, n * inc + 1, trial, np.complex64)
+        pre = gen("normal", 5, trial)
+        for name, kind, x, seedf in [("sbsssq", "s", xf, "sbsssq"), ("dbzssq", "d", xz, "dbdssq"),
+                                     ("sbcssq", "s", xc, "sbsssq")]:
+            za = binned_zeros(fold, kind); zb = binned_zeros(fold, kind)
+            p0 = pre.astype(np.float32) if kind == "s" else pre
+            sa0 = getattr(port, seedf)(fold, 5, ptr(p0), 1, 0.0, ptr(za))
+            sb0 = getattr(R, seedf)(fold, 5, ptr(p0), 1, 0.0, ptr(zb))
+            sa = getattr(port, name)(fold, n, ptr(x), inc, sa0, ptr(za))
+            sb = getattr(R, name)(fold, n, ptr(x), inc, sb0, ptr(zb))
+            assert same_state(za, zb, fold) and same_value(sa, sb), (name, n, fold, dist, inc)
+        for name, x in [("rsnrm2", xf), ("rdznrm2", xz), ("rscnrm2", xc)]:
+            assert same_value(getattr(port, name)(fold, n, ptr(x), inc),
+                              getattr(R, name)(fold, n, ptr(x), inc)), (name, n, fold, dist)
