@@ -411,6 +411,8 @@ def blas1_sweep(torch, rb):
         "dzasum": (16.0 * nc, lambda: rb.call("binnedBLAS_dbzasum", FOLD, nc, x, 1, z)),
         "zdotu": (32.0 * nc, lambda: rb.call("binnedBLAS_zbzdotu", FOLD, nc, x, 1, y, 1, zc)),
         "cdotc": (16.0 * (n // 2), lambda: rb.call("binnedBLAS_cbcdotc", FOLD, n // 2, xf, 1, yf, 1, zcf)),
+        "snrm2_ssq": (4.0 * n, lambda: rb.call("binnedBLAS_sbsssq", FOLD, n, xf, 1, 0.0, zs)),
+        "dznrm2_ssq": (16.0 * nc, lambda: rb.call("binnedBLAS_dbzssq", FOLD, nc, x, 1, 0.0, z)),
     }
     out = {}
     for name, (byts, fn) in cases.items():

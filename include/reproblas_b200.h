@@ -95,6 +95,19 @@ void reproBLAS_rcsum_sub(const int fold, const int N, const void *X, const int i
                          void *sum);
 void reproBLAS_csum_sub(const int N, const void *X, const int incX, void *sum);
 
+/* include/reproBLAS.h:35 (src/reproBLAS/rsnrm2.c): scale * sqrt(sum of squares), FP32
+ * state and scale, the square root taken in double; default fold: include/reproBLAS.h:105 */
+float reproBLAS_rsnrm2(const int fold, const int N, const float *X, const int incX);
+float reproBLAS_snrm2(const int N, const float *X, const int incX);
+/* include/reproBLAS.h:39 (src/reproBLAS/rdznrm2.c): 2-norm of complex128; default fold:
+ * include/reproBLAS.h:109 */
+double reproBLAS_rdznrm2(const int fold, const int N, const void *X, const int incX);
+double reproBLAS_dznrm2(const int N, const void *X, const int incX);
+/* include/reproBLAS.h:45 (src/reproBLAS/rscnrm2.c): 2-norm of complex64; default fold:
+ * include/reproBLAS.h:115 */
+float reproBLAS_rscnrm2(const int fold, const int N, const void *X, const int incX);
+float reproBLAS_scnrm2(const int N, const void *X, const int incX);
+
 /* include/reproBLAS.h:28 (src/reproBLAS/rdasum.c): sum of |x_i|; default fold:
  * include/reproBLAS.h:98 */
 double reproBLAS_rdasum(const int fold, const int N, const double *X, const int incX);
@@ -183,6 +196,16 @@ void binnedBLAS_zbzdotc(const int fold, const int N, const void *X, const int in
 /* include/binnedBLAS.h:76 (src/binnedBLAS/cbcsum.c -> cmcsum.ccog) */
 void binnedBLAS_cbcsum(const int fold, const int N, const void *X, const int incX,
                        float_complex_binned *Y);
+/* include/binnedBLAS.h:71 (src/binnedBLAS/sbsssq.c -> smsssq.ccog): returns the new scale */
+float binnedBLAS_sbsssq(const int fold, const int N, const float *X, const int incX,
+                        const float scaleY, float_binned *Y);
+/* include/binnedBLAS.h:60 (src/binnedBLAS/dbzssq.c -> dmzssq.ccog): squares of both
+ * components of complex128 into a real scaled state; returns the new scale */
+double binnedBLAS_dbzssq(const int fold, const int N, const void *X, const int incX,
+                         const double scaleY, double_binned *Y);
+/* include/binnedBLAS.h:80 (src/binnedBLAS/sbcssq.c -> smcssq.ccog) */
+float binnedBLAS_sbcssq(const int fold, const int N, const void *X, const int incX,
+                        const float scaleY, float_binned *Y);
 /* include/binnedBLAS.h:49 (src/binnedBLAS/dbdasum.c -> dmdasum.ccog:57-101) */
 void binnedBLAS_dbdasum(const int fold, const int N, const double *X, const int incX,
                         double_binned *Y);

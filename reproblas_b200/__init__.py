@@ -51,6 +51,15 @@ SIGNATURES = {
     "binnedBLAS_zbzsum": (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp]),
     "binnedBLAS_zbzdotc": (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp, _c_int, _c_vp]),
     "binnedBLAS_cbcsum": (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp]),
+    "reproBLAS_rsnrm2": (_c_float, [_c_int, _c_int, _c_vp, _c_int]),
+    "reproBLAS_snrm2": (_c_float, [_c_int, _c_vp, _c_int]),
+    "reproBLAS_rdznrm2": (_c_double, [_c_int, _c_int, _c_vp, _c_int]),
+    "reproBLAS_dznrm2": (_c_double, [_c_int, _c_vp, _c_int]),
+    "reproBLAS_rscnrm2": (_c_float, [_c_int, _c_int, _c_vp, _c_int]),
+    "reproBLAS_scnrm2": (_c_float, [_c_int, _c_vp, _c_int]),
+    "binnedBLAS_sbsssq": (_c_float, [_c_int, _c_int, _c_vp, _c_int, _c_float, _c_vp]),
+    "binnedBLAS_dbzssq": (_c_double, [_c_int, _c_int, _c_vp, _c_int, _c_double, _c_vp]),
+    "binnedBLAS_sbcssq": (_c_float, [_c_int, _c_int, _c_vp, _c_int, _c_float, _c_vp]),
     "reproBLAS_rdasum": (_c_double, [_c_int, _c_int, _c_vp, _c_int]),
     "reproBLAS_dasum": (_c_double, [_c_int, _c_vp, _c_int]),
     "reproBLAS_rsasum": (_c_float, [_c_int, _c_int, _c_vp, _c_int]),

@@ -273,6 +273,33 @@ bool complex_asum(char rt, int fold, int N, const void* X, int incX, void* acc, 
   return run_blas1(re) && run_blas1(im);
 }
 
+// Scaled sum of squares of the components of a complex vector into one real state
+// (dmzssq / smcssq), taken as real values like complex_asum; the second pass starts from
+// the first pass's state and scale. Returns the new scale through *scale_out (binned_dscale
+// of 1.0 for a non-finite state); with `result`, also scale * sqrt(conv).
+bool complex_ssq(char rt, int fold, int N, const void* X, int incX, void* acc, double scale_in,
+                 double* scale_out, void* result) {
+  const size_t cb = rt == 'd' ? 8 : 4;
+  if (N <= 0 || (incX == 1 && N <= INT_MAX / 2)) {
+    Blas1Req r{rt, kOpSsq, fold, N > 0 ? 2 * N : N, X, 1, nullptr, 0, acc, scale_in, scale_out,
+               result, result != nullptr};
+    return run_blas1(r);
+  }
+  if (incX < 0 || incX > INT_MAX / 2) {
+    set_error(RB_ERR_INVALID_ARG, "negative or too large stride");
+    return false;
+  }
+  double tmp[2 * kMaxFold] = {};
+  float tmpf[2 * kMaxFold] = {};
+  void* st = acc ? acc : (rt == 'd' ? (void*)tmp : (void*)tmpf);
+  double s1 = 0.0;
+  Blas1Req re{rt, kOpSsq, fold, N, X, 2 * incX, nullptr, 0, st, scale_in, &s1, nullptr, false};
+  if (!run_blas1(re)) return false;
+  Blas1Req im{rt, kOpSsq, fold, N, (const unsigned char*)X + cb, 2 * incX, nullptr, 0, st, s1,
+              scale_out, result, result != nullptr};
+  return run_blas1(im);
+}
+
 }  // namespace
 }  // namespace rb
 
@@ -343,6 +370,29 @@ void reproBLAS_csum_sub(const int N, const void* X, const int incX, void* sum) {
   reproBLAS_rcsum_sub(3, N, X, incX, sum);
 }
 
+float reproBLAS_rsnrm2(const int fold, const int N, const float* X, const int incX) {
+  float out = 0.0f;
+  Blas1Req r{'s', rb::kOpSsq, fold, N, X, incX, nullptr, 0, nullptr, 0.0, nullptr, &out, true};
+  return rb::run_blas1(r) ? out : (float)rb::qnan();
+}
+float reproBLAS_snrm2(const int N, const float* X, const int incX) {
+  return reproBLAS_rsnrm2(3, N, X, incX);
+}
+double reproBLAS_rdznrm2(const int fold, const int N, const void* X, const int incX) {
+  double out = 0.0, scl = 0.0;
+  return rb::complex_ssq('d', fold, N, X, incX, nullptr, 0.0, &scl, &out) ? out : rb::qnan();
+}
+double reproBLAS_dznrm2(const int N, const void* X, const int incX) {
+  return reproBLAS_rdznrm2(3, N, X, incX);
+}
+float reproBLAS_rscnrm2(const int fold, const int N, const void* X, const int incX) {
+  float out = 0.0f;
+  double scl = 0.0;
+  return rb::complex_ssq('s', fold, N, X, incX, nullptr, 0.0, &scl, &out) ? out : (float)rb::qnan();
+}
+float reproBLAS_scnrm2(const int N, const void* X, const int incX) {
+  return reproBLAS_rscnrm2(3, N, X, incX);
+}
 double reproBLAS_rdasum(const int fold, const int N, const double* X, const int incX) {
   return rb::value_d('d', rb::kOpAsum, fold, N, X, incX, nullptr, 0, false);
 }
@@ -400,6 +450,23 @@ void reproBLAS_cdotu_sub(const int N, const void* X, const int incX, const void*
 }
 
 // ---- binnedBLAS level ------------------------------------------------------------------------
+float binnedBLAS_sbsssq(const int fold, const int N, const float* X, const int incX,
+                        const float scaleY, float_binned* Y) {
+  double scl = rb::qnan();
+  Blas1Req r{'s', rb::kOpSsq, fold, N, X, incX, nullptr, 0, Y, scaleY, &scl, nullptr, false};
+  return rb::run_blas1(r) ? (float)scl : (float)rb::qnan();
+}
+double binnedBLAS_dbzssq(const int fold, const int N, const void* X, const int incX,
+                         const double scaleY, double_binned* Y) {
+  double scl = rb::qnan();
+  return rb::complex_ssq('d', fold, N, X, incX, Y, scaleY, &scl, nullptr) ? scl : rb::qnan();
+}
+float binnedBLAS_sbcssq(const int fold, const int N, const void* X, const int incX,
+                        const float scaleY, float_binned* Y) {
+  double scl = rb::qnan();
+  return rb::complex_ssq('s', fold, N, X, incX, Y, scaleY, &scl, nullptr) ? (float)scl
+                                                                          : (float)rb::qnan();
+}
 void binnedBLAS_dbdasum(const int fold, const int N, const double* X, const int incX,
                         double_binned* Y) {
   Blas1Req r{'d', rb::kOpAsum, fold, N, X, incX, nullptr, 0, Y, 0.0, nullptr, nullptr, false};

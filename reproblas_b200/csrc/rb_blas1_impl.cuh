@@ -50,8 +50,9 @@ template <bool GLOBAL, typename T> __device__ __forceinline__ T ldrec(const T* p
 }
 
 // ---------------------------------------------------------------------------------------
-// Sum-of-squares helpers: binned_dscale (src/binned/dscale.c:25-31) and
-// binned_dmdrescale (src/binned/dmdrescale.c:20-37).
+// Sum-of-squares helpers: binned_dscale / binned_sscale (src/binned/dscale.c:25-31,
+// sscale.c), binned_dmdrescale / binned_smsrescale (src/binned/dmdrescale.c:20-37,
+// smsrescale.c) and binned_dmdmaddsq / smsmaddsq (dmdmaddsq.c:26-41, smsmaddsq.c).
 // ---------------------------------------------------------------------------------------
 __device__ __forceinline__ double dscale_of_key(unsigned key) {
   int e = (int)(key >> 20);
@@ -60,45 +61,59 @@ __device__ __forceinline__ double dscale_of_key(unsigned key) {
   // ldexp(0.5, e - 1022) == 2^(e - 1023): biased exponent e
   return __longlong_as_double((long long)e << 52);
 }
+__device__ __forceinline__ float sscale_of_key(unsigned key) {
+  int e = (int)(key >> 23);
+  e = e < 13 ? 13 : e;
+  e -= (e - 126 - 1) % 13;
+  // ldexpf(0.5f, e - 126) == 2^(e - 127): biased exponent e
+  return __uint_as_float((unsigned)e << 23);
+}
+template <typename T> __device__ __forceinline__ T scale_of_key(unsigned key);
+template <> __device__ __forceinline__ double scale_of_key<double>(unsigned key) { return dscale_of_key(key); }
+template <> __device__ __forceinline__ float scale_of_key<float>(unsigned key) { return sscale_of_key(key); }
 
-template <int F>
-__device__ __forceinline__ void rescale(Acc<double, F>& a, double x, double scaleY) {
-  if (x == scaleY || x == 0.0 || scaleY == 0.0) return;
+__device__ __forceinline__ double bdiv(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float bdiv(float a, float b) { return __fdiv_rn(a, b); }
+
+template <typename T, int F>
+__device__ __forceinline__ void rescale(Acc<T, F>& a, T x, T scaleY) {
+  using B = BT<T>;
+  if (x == scaleY || x == T(0) || scaleY == T(0)) return;
   if (a.idx == kEmpty) {
     // dividing an all-zero state reproduces binned_dmdupdate(fold, 0.0) on it
-    a.raise_to(BT<double>::kMaxIndex);
+    a.raise_to(B::kMaxIndex);
     return;
   }
-  double r = __ddiv_rn(x, scaleY);
-  r = __dmul_rn(r, r);
+  T r = bdiv(x, scaleY);
+  r = B::mul(r, r);
   bool reset = false;
 #pragma unroll
   for (int i = 0; i < F; i++) {
     if (!reset) {
-      a.pri[i] = __ddiv_rn(a.pri[i], r);
-      if (a.pri[i] == 0.0) {
+      a.pri[i] = bdiv(a.pri[i], r);
+      if (a.pri[i] == T(0)) {
         reset = true;
         // binned_dmdupdate(fold - i, 0.0, ...) on the all-zero tail
 #pragma unroll
         for (int j = 0; j < F; j++)
-          if (j >= i) { a.pri[j] = BT<double>::bin(BT<double>::kMaxIndex + j - i); a.car[j] = 0.0; }
+          if (j >= i) { a.pri[j] = B::bin(B::kMaxIndex + j - i); a.car[j] = T(0); }
       }
     }
   }
-  a.set_idx(BT<double>::mindex(a.pri[0]));
+  a.set_idx(B::mindex(a.pri[0]));
 }
 
-// binned_dmdmaddsq (src/binned/dmdmaddsq.c:26-41): Y(scaleY) += X(scaleX)
-template <int F>
-__device__ __forceinline__ void merge_sq(Acc<double, F>& Y, double& sY, Acc<double, F> X, double sX) {
+// Y(scaleY) += X(scaleX); the scales are powers of two held as doubles
+template <typename T, int F>
+__device__ __forceinline__ void merge_sq(Acc<T, F>& Y, double& sY, Acc<T, F> X, double sX) {
   if (sX > sY) {
-    rescale(Y, sX, sY);
+    rescale(Y, (T)sX, (T)sY);
     Y.merge(X);
     sY = sX;
   } else if (sX == sY) {
     Y.merge(X);
   } else {
-    rescale(X, sY, sX);
+    rescale(X, (T)sY, (T)sX);
     Y.merge(X);
   }
 }
@@ -152,26 +167,25 @@ struct Red1 {
           a.flags |= (x[k] != x[k]) ? kNaN : kPosInf;
       return;
     }
-    if constexpr (sizeof(T) == 8) {
-      double nscl = dscale_of_key(m);
-      if (nscl > scl) {
-        if (scl > 0.0) rescale(a, nscl, scl);
-        scl = nscl;
-      }
-      double inv = __ddiv_rn(1.0, scl);
-      double v[K];
-#pragma unroll
-      for (int k = 0; k < K; k++) {
-        double t = __dmul_rn(x[k], inv);
-        v[k] = __dmul_rn(t, t);
-      }
-      a.template tile<K>(v, nv);
+    const T nscl = scale_of_key<T>(m);
+    if ((double)nscl > scl) {
+      if (scl > 0.0) rescale(a, nscl, (T)scl);
+      scl = (double)nscl;
     }
+    // x * (1/scale), squared (depositSSq.py:17-26); 1/scale is an exact power of two
+    const T inv = bdiv(T(1), (T)scl);
+    T v[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const T t = BT<T>::mul(x[k], inv);
+      v[k] = BT<T>::mul(t, t);
+    }
+    a.template tile<K>(v, nv);
   }
 
   __device__ __forceinline__ void merge(const Red1& o) {
     if (OP == kOpSsq) {
-      if constexpr (sizeof(T) == 8) merge_sq(a, scl, o.a, o.scl);
+      merge_sq(a, scl, o.a, o.scl);
     } else {
       a.merge(o.a);
     }
@@ -366,7 +380,10 @@ blas1_kernel(Blas1Args args) {
         if (OP == kOpSsq && args.sqrt_result) c = __dmul_rn(scl, __dsqrt_rn(c));  // rdnrm2.c:31
         *(double*)args.result = c;
       } else {
-        *(float*)args.result = sconv<F>(outp, outc, 1);
+        float c = sconv<F>(outp, outc, 1);
+        // rsnrm2.c: scl * sqrt(conv) with the double sqrt, then rounded to float
+        if (OP == kOpSsq && args.sqrt_result) c = __double2float_rn(__dmul_rn(scl, __dsqrt_rn((double)c)));
+        *(float*)args.result = c;
       }
     }
     *args.scratch.ticket = 0u;
@@ -637,7 +654,7 @@ cudaError_t launch_real(int op, bool vec, int grid, int block, const Blas1Args& 
   } else if (op == kOpDot) {
     if (vec) blas1_kernel<T, F, kOpDot, true><<<grid, block, 0, s>>>(a);
     else blas1_kernel<T, F, kOpDot, false><<<grid, block, 0, s>>>(a);
-  } else if (op == kOpSsq && sizeof(T) == 8) {
+  } else if (op == kOpSsq) {
     if (vec) blas1_kernel<T, F, kOpSsq, true><<<grid, block, 0, s>>>(a);
     else blas1_kernel<T, F, kOpSsq, false><<<grid, block, 0, s>>>(a);
   } else if (op == kOpAsum) {
@@ -677,8 +694,7 @@ const void* real_kernel_ptr(int op, bool vec) {
   if (op == kOpSum) return vec ? (const void*)blas1_kernel<T, F, kOpSum, true> : (const void*)blas1_kernel<T, F, kOpSum, false>;
   if (op == kOpDot) return vec ? (const void*)blas1_kernel<T, F, kOpDot, true> : (const void*)blas1_kernel<T, F, kOpDot, false>;
   if (op == kOpAsum) return vec ? (const void*)blas1_kernel<T, F, kOpAsum, true> : (const void*)blas1_kernel<T, F, kOpAsum, false>;
-  if (sizeof(T) == 8) return vec ? (const void*)blas1_kernel<T, F, kOpSsq, true> : (const void*)blas1_kernel<T, F, kOpSsq, false>;
-  return nullptr;
+  return vec ? (const void*)blas1_kernel<T, F, kOpSsq, true> : (const void*)blas1_kernel<T, F, kOpSsq, false>;
 }
 
 template <typename T, int F>

@@ -150,3 +150,83 @@ def test_asum_dots_special_values(cuda, rb, port):
             o = dev(cuda, np.zeros(2, np.float32))
             rb.call(fn, 3, n, dev(cuda, as_real(xc)), 1, dev(cuda, as_real(yc)), 1, o)
             assert same_value(host(o), want), fn
+
+
+def test_golden_ssq_more(cuda, rb, golden):
+    """FP32 and complex scaled sums of squares and the 2-norms built on them."""
+    bad = []
+    for c in golden["blas1_more"]:
+        dist, n, fold = c["dist"], c["n"], c["fold"]
+        xf = gen(dist, n, 11, np.float32)
+        xz, xc = gen_complex(dist, n, 11), gen_complex(dist, n, 11, np.complex64)
+        for name, kind, x, dt in [("sbsssq", "s", xf, np.float32), ("dbzssq", "d", as_real(xz), np.float64),
+                                  ("sbcssq", "s", as_real(xc), np.float32)]:
+            z = dev(cuda, binned_zeros(fold, kind))
+            sc = rb.call("binnedBLAS_" + name, fold, n, dev(cuda, x), 1, 0.0, z)
+            if not same_state(host(z), from_hex(c[name], dt), fold):
+                bad.append((name, dist, n, fold))
+            if not same_value(np.asarray(sc, dt), from_hex(c[name + "_scale"], dt)[0]):
+                bad.append((name + "_scale", dist, n, fold))
+        for name, x, dt in [("rsnrm2", xf, np.float32), ("rdznrm2", as_real(xz), np.float64),
+                            ("rscnrm2", as_real(xc), np.float32)]:
+            v = rb.call("reproBLAS_" + name, fold, n, dev(cuda, x), 1)
+            if not same_value(np.asarray(v, dt), from_hex(c[name], dt)[0]):
+                bad.append((name, dist, n, fold))
+    assert not bad, bad[:10]
+
+
+@pytest.mark.parametrize("fold", [2, 3, 6])
+def test_ssq_more_vs_oracle(cuda, rb, port, fold):
+    """Scaled sums of squares into scaled non-empty states, strides, offsets, device and host
+    pointers; and the 2-norms."""
+    rng = np.random.default_rng(70 + fold)
+    for n in [0, 1, 5, 64, 257, 1023, 4097, 70001]:
+        inc = int(rng.integers(1, 4))
+        off = int(rng.integers(0, 2))
+        dist = ["uniform", "normal", "loguniform", "illcond", "huge", "tiny"][n % 6]
+        m = n * inc + 2
+        bf = gen(dist, m, n + 1, np.float32)
+        bz = gen_complex(dist, m, n + 2)
+        bc = gen_complex(dist, m, n + 2, np.complex64)
+        pre = gen("normal", 4, n)
+        for name, kind, arr, seedf in [("sbsssq", "s", bf, "sbsssq"), ("dbzssq", "d", bz, "dbdssq"),
+                                       ("sbcssq", "s", bc, "sbsssq")]:
+            want = binned_zeros(fold, kind)
+            p0 = pre.astype(np.float32) if kind == "s" else pre
+            s0 = getattr(port, seedf)(fold, 4, ptr(p0), 1, 0.0, ptr(want))
+            start = want.copy()
+            sw = getattr(port, name)(fold, n, ptr(arr[off:]), inc, s0, ptr(want))
+            r = as_real(arr) if arr.dtype.kind == "c" else arr
+            step = 2 if arr.dtype.kind == "c" else 1
+            z = dev(cuda, start)
+            sg = rb.call("binnedBLAS_" + name, fold, n, dev(cuda, r)[step * off:], inc, s0, z)
+            assert same_state(host(z), want, fold) and same_value(sg, sw), (name, n, inc, off, "device")
+            zh = start.copy()
+            sh = rb.call("binnedBLAS_" + name, fold, n, np.ascontiguousarray(r[step * off:]), inc, s0, zh)
+            assert same_state(zh, want, fold) and same_value(sh, sw), (name, n, inc, off, "host")
+        for name, arr in [("rsnrm2", bf), ("rdznrm2", bz), ("rscnrm2", bc)]:
+            r = as_real(arr) if arr.dtype.kind == "c" else arr
+            step = 2 if arr.dtype.kind == "c" else 1
+            got = rb.call("reproBLAS_" + name, fold, n, dev(cuda, r)[step * off:], inc)
+            want = getattr(port, name)(fold, n, ptr(arr[off:]), inc)
+            assert same_value(got, want), (name, n, inc, off)
+
+
+def test_ssq_more_special_values(cuda, rb, port):
+    rng = np.random.default_rng(23)
+    for trial in range(60):
+        n = int(rng.integers(1, 3000))
+        x = rng.uniform(-1, 1, n)
+        for _ in range(int(rng.integers(1, 4))):
+            x[int(rng.integers(0, n))] = rng.choice([np.inf, -np.inf, np.nan])
+        xf = x.astype(np.float32)
+        assert same_value(np.float32(rb.call("reproBLAS_rsnrm2", 3, n, dev(cuda, xf), 1)),
+                          np.float32(port.rsnrm2(3, n, ptr(xf), 1)))
+        xz = np.empty(n, np.complex128)
+        xz.real = x
+        xz.imag = np.roll(x, 7)
+        assert same_value(rb.call("reproBLAS_rdznrm2", 3, n, dev(cuda, as_real(xz)), 1),
+                          port.rdznrm2(3, n, ptr(xz), 1))
+        xc = xz.astype(np.complex64)
+        assert same_value(np.float32(rb.call("reproBLAS_rscnrm2", 3, n, dev(cuda, as_real(xc)), 1)),
+                          np.float32(port.rscnrm2(3, n, ptr(xc), 1)))
