@@ -196,6 +196,23 @@ void binnedBLAS_zbzdotc(const int fold, const int N, const void *X, const int in
 /* include/binnedBLAS.h:76 (src/binnedBLAS/cbcsum.c -> cmcsum.ccog) */
 void binnedBLAS_cbcsum(const int fold, const int N, const void *X, const int incX,
                        float_complex_binned *Y);
+/* include/binnedBLAS.h:37-45 (src/binnedBLAS/damax.ccog:282-306, damaxm.ccog, samax.ccog,
+ * samaxm.ccog, zamax_sub.ccog, zamaxm_sub.ccog, camax_sub.ccog, camaxm_sub.ccog): largest
+ * |x_i| (amax) or |x_i * y_i| (amaxm); complex forms write two maxima (real and imaginary
+ * parts; for amaxm max(|xr*yr|, |xi*yi|) and max(|xi*yr|, |xr*yi|)). A NaN anywhere gives
+ * NaN (the reference's NaN result depends on the NaN's position in its SIMD lanes). */
+double binnedBLAS_damax(const int N, const double *X, const int incX);
+float binnedBLAS_samax(const int N, const float *X, const int incX);
+double binnedBLAS_damaxm(const int N, const double *X, const int incX, const double *Y,
+                         const int incY);
+float binnedBLAS_samaxm(const int N, const float *X, const int incX, const float *Y,
+                        const int incY);
+void binnedBLAS_zamax_sub(const int N, const void *X, const int incX, void *amax);
+void binnedBLAS_camax_sub(const int N, const void *X, const int incX, void *amax);
+void binnedBLAS_zamaxm_sub(const int N, const void *X, const int incX, const void *Y,
+                           const int incY, void *amaxm);
+void binnedBLAS_camaxm_sub(const int N, const void *X, const int incX, const void *Y,
+                           const int incY, void *amaxm);
 /* include/binnedBLAS.h:71 (src/binnedBLAS/sbsssq.c -> smsssq.ccog): returns the new scale */
 float binnedBLAS_sbsssq(const int fold, const int N, const float *X, const int incX,
                         const float scaleY, float_binned *Y);

@@ -1237,6 +1237,75 @@ float rbo_sbcssq(int fold, int N, const void *Xv, int incX, float scaleY, float 
 }
 
 /* ------------------------------------------------------------------------- */
+/* Largest magnitudes: src/binnedBLAS/damax.ccog:282-306 etc. (amax.py, amaxm.py)  */
+/* For finite and infinite input; with NaN the reference's result depends on its  */
+/* SIMD lane order, and the restatement returns NaN whenever one is present.       */
+/* ------------------------------------------------------------------------- */
+static double dmaxn(double m, double v) { v = fabs(v); return (isnan(m) || isnan(v)) ? NAN : (v > m ? v : m); }
+static float smaxn(float m, float v) { v = fabsf(v); return (isnan(m) || isnan(v)) ? NAN : (v > m ? v : m); }
+
+double rbo_damax(int N, const double *X, int incX) {
+  double m = 0.0;
+  for (int i = 0; i < N; i++) m = dmaxn(m, X[(size_t)i * incX]);
+  return m;
+}
+float rbo_samax(int N, const float *X, int incX) {
+  float m = 0.0f;
+  for (int i = 0; i < N; i++) m = smaxn(m, X[(size_t)i * incX]);
+  return m;
+}
+double rbo_damaxm(int N, const double *X, int incX, const double *Y, int incY) {
+  double m = 0.0;
+  for (int i = 0; i < N; i++) m = dmaxn(m, X[(size_t)i * incX] * Y[(size_t)i * incY]);
+  return m;
+}
+float rbo_samaxm(int N, const float *X, int incX, const float *Y, int incY) {
+  float m = 0.0f;
+  for (int i = 0; i < N; i++) m = smaxn(m, X[(size_t)i * incX] * Y[(size_t)i * incY]);
+  return m;
+}
+void rbo_zamax_sub(int N, const void *Xv, int incX, void *amax) {
+  const double *X = (const double *)Xv;
+  double *o = (double *)amax;
+  o[0] = o[1] = 0.0;
+  for (int i = 0; i < N; i++) {
+    o[0] = dmaxn(o[0], X[2 * (size_t)i * incX]);
+    o[1] = dmaxn(o[1], X[2 * (size_t)i * incX + 1]);
+  }
+}
+void rbo_camax_sub(int N, const void *Xv, int incX, void *amax) {
+  const float *X = (const float *)Xv;
+  float *o = (float *)amax;
+  o[0] = o[1] = 0.0f;
+  for (int i = 0; i < N; i++) {
+    o[0] = smaxn(o[0], X[2 * (size_t)i * incX]);
+    o[1] = smaxn(o[1], X[2 * (size_t)i * incX + 1]);
+  }
+}
+void rbo_zamaxm_sub(int N, const void *Xv, int incX, const void *Yv, int incY, void *amaxm) {
+  const double *X = (const double *)Xv, *Y = (const double *)Yv;
+  double *o = (double *)amaxm;
+  o[0] = o[1] = 0.0;
+  for (int i = 0; i < N; i++) {
+    double xr = X[2 * (size_t)i * incX], xi = X[2 * (size_t)i * incX + 1];
+    double yr = Y[2 * (size_t)i * incY], yi = Y[2 * (size_t)i * incY + 1];
+    o[0] = dmaxn(dmaxn(o[0], xr * yr), xi * yi);
+    o[1] = dmaxn(dmaxn(o[1], xi * yr), xr * yi);
+  }
+}
+void rbo_camaxm_sub(int N, const void *Xv, int incX, const void *Yv, int incY, void *amaxm) {
+  const float *X = (const float *)Xv, *Y = (const float *)Yv;
+  float *o = (float *)amaxm;
+  o[0] = o[1] = 0.0f;
+  for (int i = 0; i < N; i++) {
+    float xr = X[2 * (size_t)i * incX], xi = X[2 * (size_t)i * incX + 1];
+    float yr = Y[2 * (size_t)i * incY], yi = Y[2 * (size_t)i * incY + 1];
+    o[0] = smaxn(smaxn(o[0], xr * yr), xi * yi);
+    o[1] = smaxn(smaxn(o[1], xi * yr), xr * yi);
+  }
+}
+
+/* ------------------------------------------------------------------------- */
 /* BLAS2/3: src/binnedBLAS/dbdgemv.ccog:57-162, dbdgemm.ccog:61-420            */
 /* ------------------------------------------------------------------------- */
 static int is_row_major(char o) { return o == 'r' || o == 'R'; }

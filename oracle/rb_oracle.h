@@ -71,6 +71,14 @@ void   rbo_sbcasum(int fold, int N, const void *X, int incX, float *Y);
 void   rbo_zbzdotu(int fold, int N, const void *X, int incX, const void *Y, int incY, double *Z);
 void   rbo_cbcdotc(int fold, int N, const void *X, int incX, const void *Y, int incY, float *Z);
 void   rbo_cbcdotu(int fold, int N, const void *X, int incX, const void *Y, int incY, float *Z);
+double rbo_damax(int N, const double *X, int incX);
+float  rbo_samax(int N, const float *X, int incX);
+double rbo_damaxm(int N, const double *X, int incX, const double *Y, int incY);
+float  rbo_samaxm(int N, const float *X, int incX, const float *Y, int incY);
+void   rbo_zamax_sub(int N, const void *X, int incX, void *amax);
+void   rbo_camax_sub(int N, const void *X, int incX, void *amax);
+void   rbo_zamaxm_sub(int N, const void *X, int incX, const void *Y, int incY, void *amaxm);
+void   rbo_camaxm_sub(int N, const void *X, int incX, const void *Y, int incY, void *amaxm);
 float  rbo_sscale(float x);
 float  rbo_sbsssq(int fold, int N, const float *X, int incX, float scaleY, float *Y);
 double rbo_dbzssq(int fold, int N, const void *X, int incX, double scaleY, double *Y);

@@ -51,6 +51,14 @@ SIGNATURES = {
     "binnedBLAS_zbzsum": (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp]),
     "binnedBLAS_zbzdotc": (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp, _c_int, _c_vp]),
     "binnedBLAS_cbcsum": (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp]),
+    "binnedBLAS_damax": (_c_double, [_c_int, _c_vp, _c_int]),
+    "binnedBLAS_samax": (_c_float, [_c_int, _c_vp, _c_int]),
+    "binnedBLAS_damaxm": (_c_double, [_c_int, _c_vp, _c_int, _c_vp, _c_int]),
+    "binnedBLAS_samaxm": (_c_float, [_c_int, _c_vp, _c_int, _c_vp, _c_int]),
+    "binnedBLAS_zamax_sub": (None, [_c_int, _c_vp, _c_int, _c_vp]),
+    "binnedBLAS_camax_sub": (None, [_c_int, _c_vp, _c_int, _c_vp]),
+    "binnedBLAS_zamaxm_sub": (None, [_c_int, _c_vp, _c_int, _c_vp, _c_int, _c_vp]),
+    "binnedBLAS_camaxm_sub": (None, [_c_int, _c_vp, _c_int, _c_vp, _c_int, _c_vp]),
     "reproBLAS_rsnrm2": (_c_float, [_c_int, _c_int, _c_vp, _c_int]),
     "reproBLAS_snrm2": (_c_float, [_c_int, _c_vp, _c_int]),
     "reproBLAS_rdznrm2": (_c_double, [_c_int, _c_int, _c_vp, _c_int]),

@@ -37,6 +37,14 @@ _SIGS = {
     "zbzdotu": (None, [c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp]),
     "cbcdotc": (None, [c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp]),
     "cbcdotu": (None, [c_int, c_int, c_vp, c_int, c_vp, c_int, c_vp]),
+    "damax": (c_double, [c_int, c_vp, c_int]),
+    "samax": (c_float, [c_int, c_vp, c_int]),
+    "damaxm": (c_double, [c_int, c_vp, c_int, c_vp, c_int]),
+    "samaxm": (c_float, [c_int, c_vp, c_int, c_vp, c_int]),
+    "zamax_sub": (None, [c_int, c_vp, c_int, c_vp]),
+    "camax_sub": (None, [c_int, c_vp, c_int, c_vp]),
+    "zamaxm_sub": (None, [c_int, c_vp, c_int, c_vp, c_int, c_vp]),
+    "camaxm_sub": (None, [c_int, c_vp, c_int, c_vp, c_int, c_vp]),
     "sbsssq": (c_float, [c_int, c_int, c_vp, c_int, c_float, c_vp]),
     "dbzssq": (c_double, [c_int, c_int, c_vp, c_int, c_double, c_vp]),
     "sbcssq": (c_float, [c_int, c_int, c_vp, c_int, c_float, c_vp]),
@@ -96,6 +104,10 @@ _REF_NAMES = {
     "rzdotu_sub": "reproBLAS_rzdotu_sub", "rcdotc_sub": "reproBLAS_rcdotc_sub",
     "rcdotu_sub": "reproBLAS_rcdotu_sub",
     "sbsssq": "binnedBLAS_sbsssq", "dbzssq": "binnedBLAS_dbzssq", "sbcssq": "binnedBLAS_sbcssq",
+    "damax": "binnedBLAS_damax", "samax": "binnedBLAS_samax", "damaxm": "binnedBLAS_damaxm",
+    "samaxm": "binnedBLAS_samaxm", "zamax_sub": "binnedBLAS_zamax_sub",
+    "camax_sub": "binnedBLAS_camax_sub", "zamaxm_sub": "binnedBLAS_zamaxm_sub",
+    "camaxm_sub": "binnedBLAS_camaxm_sub",
     "rsnrm2": "reproBLAS_rsnrm2", "rdznrm2": "reproBLAS_rdznrm2", "rscnrm2": "reproBLAS_rscnrm2",
     "dbdbadd": "binned_dbdbadd", "dbdconv": "binned_dbdconv", "ddbconv": "binned_ddbconv",
     "dbdbaddsq": "binned_dbdbaddsq", "dbbound": "binned_dbbound", "dscale": "binned_dscale",

@@ -230,3 +230,42 @@ def test_ssq_more_special_values(cuda, rb, port):
         xc = xz.astype(np.complex64)
         assert same_value(np.float32(rb.call("reproBLAS_rscnrm2", 3, n, dev(cuda, as_real(xc)), 1)),
                           np.float32(port.rscnrm2(3, n, ptr(xc), 1)))
+
+
+def test_amax_family(cuda, rb, port):
+    """binnedBLAS_[dszc]amax and amaxm: device and host pointers, strides, infinities and
+    NaN (NaN anywhere gives NaN, as in the oracle)."""
+    rng = np.random.default_rng(31)
+    for trial in range(40):
+        n = int(rng.integers(0, 70000)) if trial % 4 else int(rng.integers(0, 70))
+        inc = int(rng.integers(1, 4))
+        dist = ["uniform", "normal", "loguniform", "illcond"][trial % 4]
+        x, y = gen(dist, n * inc + 1, trial), gen(dist, n * inc + 1, trial + 1)
+        if n and trial % 3 == 0:
+            x[int(rng.integers(0, n)) * inc] = [np.inf, -np.inf, np.nan][trial % 9 // 3]
+        xf, yf = x.astype(np.float32), y.astype(np.float32)
+        xz, yz = gen_complex(dist, n * inc + 1, trial), gen_complex(dist, n * inc + 1, trial + 2)
+        if n and trial % 3 == 1:
+            xz[int(rng.integers(0, n)) * inc] = complex(np.nan, 1.0)
+        xc, yc = xz.astype(np.complex64), yz.astype(np.complex64)
+        for src in ("dev", "host"):
+            d = (lambda a: dev(cuda, as_real(a) if a.dtype.kind == "c" else a)) if src == "dev" else \
+                (lambda a: np.ascontiguousarray(as_real(a) if a.dtype.kind == "c" else a))
+            assert same_value(rb.call("binnedBLAS_damax", n, d(x), inc), port.damax(n, ptr(x), inc))
+            assert same_value(np.float32(rb.call("binnedBLAS_samax", n, d(xf), inc)),
+                              np.float32(port.samax(n, ptr(xf), inc)))
+            assert same_value(rb.call("binnedBLAS_damaxm", n, d(x), inc, d(y), inc),
+                              port.damaxm(n, ptr(x), inc, ptr(y), inc))
+            assert same_value(np.float32(rb.call("binnedBLAS_samaxm", n, d(xf), inc, d(yf), inc)),
+                              np.float32(port.samaxm(n, ptr(xf), inc, ptr(yf), inc)))
+            for name, a, b, dt in [("zamax_sub", xz, None, np.float64), ("camax_sub", xc, None, np.float32),
+                                   ("zamaxm_sub", xz, yz, np.float64), ("camaxm_sub", xc, yc, np.float32)]:
+                want = np.zeros(2, dt)
+                pargs = [n, ptr(a), inc] + ([ptr(b), inc] if b is not None else [])
+                getattr(port, name)(*pargs, ptr(want))
+                got = np.zeros(2, dt)
+                gargs = [n, d(a), inc] + ([d(b), inc] if b is not None else [])
+                out = dev(cuda, got) if src == "dev" else got
+                rb.call("binnedBLAS_" + name, *gargs, out)
+                got = host(out) if src == "dev" else got
+                assert same_value(got, want), (name, n, inc, src)

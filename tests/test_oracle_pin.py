@@ -349,3 +349,45 @@ def test_port_matches_reference_live_ssq_more(port, inc):
         for name, x in [("rsnrm2", xf), ("rdznrm2", xz), ("rscnrm2", xc)]:
             assert same_value(getattr(port, name)(fold, n, ptr(x), inc),
                               getattr(R, name)(fold, n, ptr(x), inc)), (name, n, fold, dist)
+
+
+@needs_ref
+def test_port_matches_reference_amax(port):
+    """Largest magnitudes on finite and infinite input (the reference's NaN result depends on
+    its SIMD lane order; the restatement and the GPU give NaN)."""
+    R = ref()
+    rng = np.random.default_rng(77)
+    for trial in range(60):
+        n = int(rng.integers(0, 4000))
+        inc = int(rng.integers(1, 4))
+        dist = ["uniform", "normal", "loguniform", "illcond", "huge", "tiny"][trial % 6]
+        x, y = gen(dist, n * inc + 1, trial), gen(dist, n * inc + 1, trial + 1)
+        if trial % 5 == 0 and n > 0:
+            x[int(rng.integers(0, n)) * inc] = rng.choice([np.inf, -np.inf])
+        with np.errstate(all="ignore"):
+            xf, yf = x.astype(np.float32), y.astype(np.float32)
+            xz, yz = gen_complex(dist, n * inc + 1, trial), gen_complex(dist, n * inc + 1, trial + 2)
+            xc, yc = xz.astype(np.complex64), yz.astype(np.complex64)
+            # products that are NaN (an infinity times zero) make the reference's result
+            # depend on lane order; those inputs are left out
+            nan_free = lambda *ps: not any(np.isnan(p).any() for p in ps)
+            okd = nan_free(x * y)
+            okf = nan_free(xf * yf)
+            okz = nan_free(xz.real * yz.real, xz.imag * yz.imag, xz.imag * yz.real, xz.real * yz.imag)
+            okc = nan_free(xc.real * yc.real, xc.imag * yc.imag, xc.imag * yc.real, xc.real * yc.imag)
+        assert same_value(port.damax(n, ptr(x), inc), R.damax(n, ptr(x), inc))
+        assert same_value(port.samax(n, ptr(xf), inc), R.samax(n, ptr(xf), inc))
+        if okd:
+            assert same_value(port.damaxm(n, ptr(x), inc, ptr(y), inc), R.damaxm(n, ptr(x), inc, ptr(y), inc))
+        if okf:
+            assert same_value(port.samaxm(n, ptr(xf), inc, ptr(yf), inc), R.samaxm(n, ptr(xf), inc, ptr(yf), inc))
+        for name, a, b, dt, ok in [("zamax_sub", xz, None, np.float64, True),
+                                   ("camax_sub", xc, None, np.float32, True),
+                                   ("zamaxm_sub", xz, yz, np.float64, okz),
+                                   ("camaxm_sub", xc, yc, np.float32, okc)]:
+            if not ok:
+                continue
+            oa = np.zeros(2, dt); ob = np.zeros(2, dt)
+            args = [n, ptr(a), inc] + ([ptr(b), inc] if b is not None else [])
+            getattr(port, name)(*args, ptr(oa)); getattr(R, name)(*args, ptr(ob))
+            assert same_value(oa, ob), (name, n, inc, dist)
