@@ -166,6 +166,59 @@ void reproBLAS_dgemm(const char Order, const char TransA, const char TransB, con
                      const int lda, const double *B, const int ldb, const double beta,
                      double *C, const int ldc);
 
+/* FP32 real and FP64 / FP32 complex gemv and gemm: include/reproBLAS.h:61-93 (fold
+ * argument) and 130-161 (fold 3); src/reproBLAS/rsgemv.c:35, rsgemm.c:41-105, rzgemv.c:35-93,
+ * rzgemm.c:41-110, rcgemv.c:35-93, rcgemm.c:41-110 and the fold-3 wrappers sgemv.c:32,
+ * sgemm.c:38, zgemv.c:32, zgemm.c:38, cgemv.c:32, cgemm.c:38.
+ * Same forms as reproBLAS_rdgemv / rdgemm, with float or complex elements: complex arrays
+ * are interleaved (re, im) pairs, strides and leading dimensions count complex elements, and
+ * complex alpha / beta point to two reals in host memory. TransA / TransB 'c'/'C' (any
+ * character other than n/N/t/T) is the conjugate transpose for complex elements. alpha
+ * multiplies x (gemv) or op(A) (gemm, after A's conjugation); beta*y is formed as
+ * (yr*br - yi*bi, yr*bi + yi*br). Column-major conjugate-transpose gemv computes the full
+ * A^H x (the reference cuts its blocks by N where M is meant, zbzgemv.ccog:214-218, and
+ * agrees with this only for M == N). */
+void reproBLAS_rsgemv(const int fold, const char Order, const char TransA, const int M,
+                      const int N, const float alpha, const float *A, const int lda,
+                      const float *X, const int incX, const float beta, float *Y,
+                      const int incY);
+void reproBLAS_sgemv(const char Order, const char TransA, const int M, const int N,
+                     const float alpha, const float *A, const int lda, const float *X,
+                     const int incX, const float beta, float *Y, const int incY);
+void reproBLAS_rsgemm(const int fold, const char Order, const char TransA, const char TransB,
+                      const int M, const int N, const int K, const float alpha, const float *A,
+                      const int lda, const float *B, const int ldb, const float beta, float *C,
+                      const int ldc);
+void reproBLAS_sgemm(const char Order, const char TransA, const char TransB, const int M,
+                     const int N, const int K, const float alpha, const float *A, const int lda,
+                     const float *B, const int ldb, const float beta, float *C, const int ldc);
+void reproBLAS_rzgemv(const int fold, const char Order, const char TransA, const int M,
+                      const int N, const void *alpha, const void *A, const int lda,
+                      const void *X, const int incX, const void *beta, void *Y, const int incY);
+void reproBLAS_zgemv(const char Order, const char TransA, const int M, const int N,
+                     const void *alpha, const void *A, const int lda, const void *X,
+                     const int incX, const void *beta, void *Y, const int incY);
+void reproBLAS_rzgemm(const int fold, const char Order, const char TransA, const char TransB,
+                      const int M, const int N, const int K, const void *alpha, const void *A,
+                      const int lda, const void *B, const int ldb, const void *beta, void *C,
+                      const int ldc);
+void reproBLAS_zgemm(const char Order, const char TransA, const char TransB, const int M,
+                     const int N, const int K, const void *alpha, const void *A, const int lda,
+                     const void *B, const int ldb, const void *beta, void *C, const int ldc);
+void reproBLAS_rcgemv(const int fold, const char Order, const char TransA, const int M,
+                      const int N, const void *alpha, const void *A, const int lda,
+                      const void *X, const int incX, const void *beta, void *Y, const int incY);
+void reproBLAS_cgemv(const char Order, const char TransA, const int M, const int N,
+                     const void *alpha, const void *A, const int lda, const void *X,
+                     const int incX, const void *beta, void *Y, const int incY);
+void reproBLAS_rcgemm(const int fold, const char Order, const char TransA, const char TransB,
+                      const int M, const int N, const int K, const void *alpha, const void *A,
+                      const int lda, const void *B, const int ldb, const void *beta, void *C,
+                      const int ldc);
+void reproBLAS_cgemm(const char Order, const char TransA, const char TransB, const int M,
+                     const int N, const int K, const void *alpha, const void *A, const int lda,
+                     const void *B, const int ldb, const void *beta, void *C, const int ldc);
+
 /* ------------------------------------------------------------------------------------
  * binnedBLAS level: add into a caller-owned binned accumulator (resumable state).
  * include/binnedBLAS.h
@@ -257,6 +310,35 @@ void binnedBLAS_dbdgemm(const int fold, const char Order, const char TransA, con
                         const int M, const int N, const int K, const double alpha,
                         const double *A, const int lda, const double *B, const int ldb,
                         double_binned *C, const int ldc);
+
+/* include/binnedBLAS.h:99-133 (src/binnedBLAS/sbsgemv.ccog:57-162, sbsgemm.ccog:61-420,
+ * zbzgemv.ccog:57-229, zbzgemm.ccog:61-879, cbcgemv.ccog:57-229, cbcgemm.ccog:61-879): the
+ * binned forms of the gemv / gemm above; Y / C are binned states (float_binned 2*fold floats,
+ * double_complex_binned 4*fold doubles, float_complex_binned 4*fold floats, strides in
+ * states), added to in place. */
+void binnedBLAS_sbsgemv(const int fold, const char Order, const char TransA, const int M,
+                        const int N, const float alpha, const float *A, const int lda,
+                        const float *X, const int incX, float_binned *Y, const int incY);
+void binnedBLAS_sbsgemm(const int fold, const char Order, const char TransA, const char TransB,
+                        const int M, const int N, const int K, const float alpha,
+                        const float *A, const int lda, const float *B, const int ldb,
+                        float_binned *C, const int ldc);
+void binnedBLAS_zbzgemv(const int fold, const char Order, const char TransA, const int M,
+                        const int N, const void *alpha, const void *A, const int lda,
+                        const void *X, const int incX, double_complex_binned *Y,
+                        const int incY);
+void binnedBLAS_zbzgemm(const int fold, const char Order, const char TransA, const char TransB,
+                        const int M, const int N, const int K, const void *alpha,
+                        const void *A, const int lda, const void *B, const int ldb,
+                        double_complex_binned *C, const int ldc);
+void binnedBLAS_cbcgemv(const int fold, const char Order, const char TransA, const int M,
+                        const int N, const void *alpha, const void *A, const int lda,
+                        const void *X, const int incX, float_complex_binned *Y,
+                        const int incY);
+void binnedBLAS_cbcgemm(const int fold, const char Order, const char TransA, const char TransB,
+                        const int M, const int N, const int K, const void *alpha,
+                        const void *A, const int lda, const void *B, const int ldb,
+                        float_complex_binned *C, const int ldc);
 
 /* ------------------------------------------------------------------------------------
  * Reproducible dgemm on the tensor cores through int8 slices (no reference counterpart;

@@ -1620,3 +1620,282 @@ double rbo_exact_dot(int N, const double *X, int incX, const double *Y, int incY
   }
   return xacc_round(acc);
 }
+
+/* ------------------------------------------------------------------------- */
+/* gemv / gemm of FP32 real and FP64 / FP32 complex elements                   */
+/* (src/binnedBLAS/sbsgemv.ccog, zbzgemv.ccog, cbcgemv.ccog, sbsgemm.ccog,     */
+/* zbzgemm.ccog, cbcgemm.ccog; src/reproBLAS/r[szc]gem[mv].c)                  */
+/* Each output entry is restated as one dot product over its whole length:    */
+/* the binned state depends only on the deposited values, so the reference's   */
+/* blocking of that dot (X_BLOCK / XT_BLOCK) changes no bit.                   */
+/* ------------------------------------------------------------------------- */
+static int is_plain_trans(char t) { return t == 't' || t == 'T'; }
+
+/* src/binned/smsconv.c: setzero + smsadd (update, deposit, renorm) */
+void rbo_sbsconv(int fold, float x, float *Y) {
+  memset(Y, 0, 2 * (size_t)fold * sizeof(float));
+  rbo_smsupdate(fold, x, Y, 1, Y + fold, 1);
+  rbo_smsdeposit(fold, x, Y, 1);
+  rbo_smrenorm(fold, Y, 1, Y + fold, 1);
+}
+
+/* src/binned/zmzconv.c: each component through dmdconv with its stride-2 view */
+void rbo_zbzconv(int fold, const double *x, double *Y) {
+  memset(Y, 0, 4 * (size_t)fold * sizeof(double));
+  for (int c = 0; c < 2; c++) {
+    rbo_dmdupdate(fold, x[c], Y + c, 2, Y + 2 * fold + c, 2);
+    rbo_dmddeposit(fold, x[c], Y + c, 2);
+    rbo_dmrenorm(fold, Y + c, 2, Y + 2 * fold + c, 2);
+  }
+}
+
+/* src/binned/cmcconv.c */
+void rbo_cbcconv(int fold, const float *x, float *Y) {
+  memset(Y, 0, 4 * (size_t)fold * sizeof(float));
+  for (int c = 0; c < 2; c++) {
+    rbo_smsupdate(fold, x[c], Y + c, 2, Y + 2 * fold + c, 2);
+    rbo_smsdeposit(fold, x[c], Y + c, 2);
+    rbo_smrenorm(fold, Y + c, 2, Y + 2 * fold + c, 2);
+  }
+}
+
+/* sbsgemv.ccog:57-162: alpha scales x (fl(x*alpha)); column-major is row-major with the
+ * transpose flipped. */
+void rbo_sbsgemv(int fold, char Order, char TransA, int M, int N, float alpha, const float *A,
+                 int lda, const float *X, int incX, float *Y, int incY) {
+  if (M == 0 || N == 0 || alpha == 0.0f) return;
+  if (!is_row_major(Order)) {
+    rbo_sbsgemv(fold, 'r', is_notrans(TransA) ? 't' : 'n', N, M, alpha, A, lda, X, incX, Y, incY);
+    return;
+  }
+  int nt = is_notrans(TransA);
+  int lenx = nt ? N : M, leny = nt ? M : N;
+  float *bx = (float *)malloc((size_t)lenx * sizeof(float));
+  float *col = (float *)malloc((size_t)lenx * sizeof(float));
+  for (int j = 0; j < lenx; j++) bx[j] = alpha == 1.0f ? X[(size_t)j * incX] : X[(size_t)j * incX] * alpha;
+  for (int i = 0; i < leny; i++) {
+    float *acc = Y + (size_t)i * incY * 2 * fold;
+    if (nt) {
+      rbo_sbsdot(fold, N, A + (size_t)i * lda, 1, bx, 1, acc);
+    } else {
+      for (int j = 0; j < M; j++) col[j] = A[(size_t)j * lda + i];
+      rbo_sbsdot(fold, M, col, 1, bx, 1, acc);
+    }
+  }
+  free(col);
+  free(bx);
+}
+
+/* zbzgemv.ccog:57-229 / cbcgemv.ccog:57-229 for complex elements of type T (double or
+ * float), dot routines DOTU / DOTC. bx = fl(alpha*x) as (xr*ar - xi*ai, xr*ai + xi*ar)
+ * (zbzgemv.ccog:91-94). Stored row-major view: Rs x Cs; an output is either the dot of a
+ * stored row (row-major NoTrans, column-major Trans / ConjTrans) or of a stored column
+ * (row-major Trans / ConjTrans, column-major NoTrans); ConjTrans conjugates A (zbzdotc).
+ * Column-major ConjTrans takes the whole column of length M (the reference's blocks use
+ * N - j there, zbzgemv.ccog:218, which agrees only for M == N). */
+#define RBO_XGEMV(NAME, T, DOTU, DOTC)                                                         \
+  void NAME(int fold, char Order, char TransA, int M, int N, const void *alpha, const void *A, \
+            int lda, const void *X, int incX, T *Y, int incY) {                                \
+    const T *al = (const T *)alpha, *a = (const T *)A, *x = (const T *)X;                      \
+    if (M == 0 || N == 0 || (al[0] == 0 && al[1] == 0)) return;                               \
+    int row = is_row_major(Order), nt = is_notrans(TransA);                                    \
+    int conj = !nt && !is_plain_trans(TransA);                                                 \
+    int Rs = row ? M : N, Cs = row ? N : M;                                                    \
+    int rows_form = row ? nt : !nt;                                                            \
+    int lenx = rows_form ? Cs : Rs, leny = rows_form ? Rs : Cs;                                \
+    int one = al[0] == 1 && al[1] == 0;                                                        \
+    T *bx = (T *)malloc(2 * (size_t)lenx * sizeof(T));                                         \
+    T *vec = (T *)malloc(2 * (size_t)lenx * sizeof(T));                                        \
+    for (int j = 0; j < lenx; j++) {                                                           \
+      T xr = x[2 * (size_t)j * incX], xi = x[2 * (size_t)j * incX + 1];                        \
+      bx[2 * j] = one ? xr : xr * al[0] - xi * al[1];                                          \
+      bx[2 * j + 1] = one ? xi : xr * al[1] + xi * al[0];                                      \
+    }                                                                                          \
+    for (int i = 0; i < leny; i++) {                                                           \
+      T *acc = Y + (size_t)i * incY * 4 * fold;                                                \
+      if (rows_form) {                                                                         \
+        memcpy(vec, a + 2 * (size_t)i * lda, 2 * (size_t)lenx * sizeof(T));                    \
+      } else {                                                                                 \
+        for (int j = 0; j < lenx; j++) {                                                       \
+          vec[2 * j] = a[2 * ((size_t)j * lda + i)];                                           \
+          vec[2 * j + 1] = a[2 * ((size_t)j * lda + i) + 1];                                   \
+        }                                                                                      \
+      }                                                                                        \
+      if (conj) DOTC(fold, lenx, vec, 1, bx, 1, acc);                                          \
+      else DOTU(fold, lenx, vec, 1, bx, 1, acc);                                               \
+    }                                                                                          \
+    free(vec);                                                                                 \
+    free(bx);                                                                                  \
+  }
+RBO_XGEMV(rbo_zbzgemv, double, rbo_zbzdotu, rbo_zbzdotc)
+RBO_XGEMV(rbo_cbcgemv, float, rbo_cbcdotu, rbo_cbcdotc)
+
+/* sbsgemm.ccog:61-420: C_ij accumulates fl(fl(alpha*A_ik) * B_kj), alpha scaling A */
+void rbo_sbsgemm(int fold, char Order, char TransA, char TransB, int M, int N, int K,
+                 float alpha, const float *A, int lda, const float *B, int ldb, float *C,
+                 int ldc) {
+  if (M == 0 || N == 0 || K == 0 || alpha == 0.0f) return;
+  int row = is_row_major(Order);
+  int ta = !is_notrans(TransA), tb = !is_notrans(TransB);
+  float *arow = (float *)malloc((size_t)K * sizeof(float));
+  float *bcol = (float *)malloc((size_t)K * sizeof(float));
+  for (int i = 0; i < M; i++) {
+    for (int k = 0; k < K; k++) {
+      float a;
+      if (row) a = ta ? A[(size_t)k * lda + i] : A[(size_t)i * lda + k];
+      else     a = ta ? A[(size_t)i * lda + k] : A[(size_t)k * lda + i];
+      arow[k] = alpha == 1.0f ? a : a * alpha;
+    }
+    for (int j = 0; j < N; j++) {
+      for (int k = 0; k < K; k++) {
+        if (row) bcol[k] = tb ? B[(size_t)j * ldb + k] : B[(size_t)k * ldb + j];
+        else     bcol[k] = tb ? B[(size_t)k * ldb + j] : B[(size_t)j * ldb + k];
+      }
+      float *acc = row ? C + ((size_t)i * ldc + j) * 2 * fold : C + ((size_t)j * ldc + i) * 2 * fold;
+      rbo_sbsdot(fold, K, arow, 1, bcol, 1, acc);
+    }
+  }
+  free(bcol);
+  free(arow);
+}
+
+/* zbzgemm.ccog:61-879 / cbcgemm.ccog:61-879: op(A) is conjugated for ConjTrans and then
+ * multiplied by alpha as (ar*alr - ai*ali, ar*ali + ai*alr) (zbzgemm.ccog:99-100,360-361);
+ * C_ij accumulates dotu(op(A) row, op(B) column), or dotc(op(B) column, op(A) row) when B is
+ * conjugate-transposed (zbzgemm.ccog:154,290). */
+#define RBO_XGEMM(NAME, T, DOTU, DOTC)                                                         \
+  void NAME(int fold, char Order, char TransA, char TransB, int M, int N, int K,               \
+            const void *alpha, const void *A, int lda, const void *B, int ldb, T *C, int ldc) {  \
+    const T *al = (const T *)alpha, *a = (const T *)A, *b = (const T *)B;                      \
+    if (M == 0 || N == 0 || K == 0 || (al[0] == 0 && al[1] == 0)) return;                     \
+    int row = is_row_major(Order);                                                             \
+    int ta = !is_notrans(TransA), tb = !is_notrans(TransB);                                    \
+    int ca = ta && !is_plain_trans(TransA), cb = tb && !is_plain_trans(TransB);                \
+    int one = al[0] == 1 && al[1] == 0;                                                        \
+    T *arow = (T *)malloc(2 * (size_t)K * sizeof(T));                                          \
+    T *bcol = (T *)malloc(2 * (size_t)K * sizeof(T));                                          \
+    for (int i = 0; i < M; i++) {                                                              \
+      for (int k = 0; k < K; k++) {                                                            \
+        size_t o;                                                                              \
+        if (row) o = ta ? (size_t)k * lda + i : (size_t)i * lda + k;                           \
+        else     o = ta ? (size_t)i * lda + k : (size_t)k * lda + i;                           \
+        T ar = a[2 * o], ai = ca ? -a[2 * o + 1] : a[2 * o + 1];                               \
+        arow[2 * k] = one ? ar : ar * al[0] - ai * al[1];                                      \
+        arow[2 * k + 1] = one ? ai : ar * al[1] + ai * al[0];                                  \
+      }                                                                                        \
+      for (int j = 0; j < N; j++) {                                                            \
+        for (int k = 0; k < K; k++) {                                                          \
+          size_t o;                                                                            \
+          if (row) o = tb ? (size_t)j * ldb + k : (size_t)k * ldb + j;                         \
+          else     o = tb ? (size_t)k * ldb + j : (size_t)j * ldb + k;                         \
+          bcol[2 * k] = b[2 * o];                                                              \
+          bcol[2 * k + 1] = b[2 * o + 1];                                                      \
+        }                                                                                      \
+        T *acc = row ? C + ((size_t)i * ldc + j) * 4 * fold : C + ((size_t)j * ldc + i) * 4 * fold; \
+        if (cb) DOTC(fold, K, bcol, 1, arow, 1, acc);                                          \
+        else DOTU(fold, K, arow, 1, bcol, 1, acc);                                             \
+      }                                                                                        \
+    }                                                                                          \
+    free(bcol);                                                                                \
+    free(arow);                                                                                \
+  }
+RBO_XGEMM(rbo_zbzgemm, double, rbo_zbzdotu, rbo_zbzdotc)
+RBO_XGEMM(rbo_cbcgemm, float, rbo_cbcdotu, rbo_cbcdotc)
+
+/* rsgemv.c:35-87: Y <- conv(binned(beta*Y) + ...) (beta 0: empty; beta 1: binned(Y)) */
+void rbo_rsgemv(int fold, char Order, char TransA, int M, int N, float alpha, const float *A,
+                int lda, const float *X, int incX, float beta, float *Y, int incY) {
+  if (N == 0 || M == 0) return;
+  int leny = is_notrans(TransA) ? M : N;
+  size_t nb = 2 * (size_t)fold;
+  float *YI = (float *)calloc((size_t)leny * nb, sizeof(float));
+  if (beta != 0.0f)
+    for (int i = 0; i < leny; i++)
+      rbo_sbsconv(fold, beta == 1.0f ? Y[(size_t)i * incY] : Y[(size_t)i * incY] * beta, YI + i * nb);
+  rbo_sbsgemv(fold, Order, TransA, M, N, alpha, A, lda, X, incX, YI, 1);
+  for (int i = 0; i < leny; i++) Y[(size_t)i * incY] = rbo_ssbconv(fold, YI + i * nb);
+  free(YI);
+}
+
+/* rsgemm.c:41-105 */
+void rbo_rsgemm(int fold, char Order, char TransA, char TransB, int M, int N, int K,
+                float alpha, const float *A, int lda, const float *B, int ldb, float beta,
+                float *C, int ldc) {
+  if (M == 0 || N == 0) return;
+  int row = is_row_major(Order);
+  size_t nb = 2 * (size_t)fold;
+  float *CI = (float *)calloc((size_t)M * N * nb, sizeof(float));
+  int ldci = row ? N : M;
+  for (int i = 0; i < M; i++)
+    for (int j = 0; j < N; j++) {
+      size_t c = row ? (size_t)i * ldc + j : (size_t)j * ldc + i;
+      size_t ci = row ? (size_t)i * ldci + j : (size_t)j * ldci + i;
+      if (beta != 0.0f) rbo_sbsconv(fold, beta == 1.0f ? C[c] : C[c] * beta, CI + ci * nb);
+    }
+  rbo_sbsgemm(fold, Order, TransA, TransB, M, N, K, alpha, A, lda, B, ldb, CI, ldci);
+  for (int i = 0; i < M; i++)
+    for (int j = 0; j < N; j++) {
+      size_t c = row ? (size_t)i * ldc + j : (size_t)j * ldc + i;
+      size_t ci = row ? (size_t)i * ldci + j : (size_t)j * ldci + i;
+      C[c] = rbo_ssbconv(fold, CI + ci * nb);
+    }
+  free(CI);
+}
+
+/* rzgemv.c:35-93 / rcgemv.c:35-93: beta*y as (yr*br - yi*bi, yr*bi + yi*br) */
+#define RBO_RXGEMV(NAME, T, CONV, GEMV, OUT)                                                   \
+  void NAME(int fold, char Order, char TransA, int M, int N, const void *alpha, const void *A, \
+            int lda, const void *X, int incX, const void *beta, void *Y, int incY) {           \
+    if (N == 0 || M == 0) return;                                                              \
+    const T *bt = (const T *)beta;                                                             \
+    T *y = (T *)Y;                                                                             \
+    int leny = is_notrans(TransA) ? M : N;                                                     \
+    size_t nb = 4 * (size_t)fold;                                                              \
+    T *YI = (T *)calloc((size_t)leny * nb, sizeof(T));                                         \
+    if (!(bt[0] == 0 && bt[1] == 0))                                                           \
+      for (int i = 0; i < leny; i++) {                                                         \
+        T yr = y[2 * (size_t)i * incY], yi = y[2 * (size_t)i * incY + 1], v[2];               \
+        if (bt[0] == 1 && bt[1] == 0) { v[0] = yr; v[1] = yi; }                                \
+        else { v[0] = yr * bt[0] - yi * bt[1]; v[1] = yr * bt[1] + yi * bt[0]; }              \
+        CONV(fold, v, YI + i * nb);                                                            \
+      }                                                                                        \
+    GEMV(fold, Order, TransA, M, N, alpha, A, lda, X, incX, YI, 1);                            \
+    for (int i = 0; i < leny; i++) OUT(fold, YI + i * nb, y + 2 * (size_t)i * incY);           \
+    free(YI);                                                                                  \
+  }
+RBO_RXGEMV(rbo_rzgemv, double, rbo_zbzconv, rbo_zbzgemv, zconv)
+RBO_RXGEMV(rbo_rcgemv, float, rbo_cbcconv, rbo_cbcgemv, cconv)
+
+/* rzgemm.c:41-110 / rcgemm.c:41-110 */
+#define RBO_RXGEMM(NAME, T, CONV, GEMM, OUT)                                                   \
+  void NAME(int fold, char Order, char TransA, char TransB, int M, int N, int K,               \
+            const void *alpha, const void *A, int lda, const void *B, int ldb,                 \
+            const void *beta, void *C, int ldc) {                                              \
+    if (M == 0 || N == 0) return;                                                              \
+    const T *bt = (const T *)beta;                                                             \
+    T *cv = (T *)C;                                                                            \
+    int row = is_row_major(Order);                                                             \
+    size_t nb = 4 * (size_t)fold;                                                              \
+    T *CI = (T *)calloc((size_t)M * N * nb, sizeof(T));                                        \
+    int ldci = row ? N : M;                                                                    \
+    for (int i = 0; i < M; i++)                                                                \
+      for (int j = 0; j < N; j++) {                                                            \
+        size_t c = row ? (size_t)i * ldc + j : (size_t)j * ldc + i;                            \
+        size_t ci = row ? (size_t)i * ldci + j : (size_t)j * ldci + i;                         \
+        if (bt[0] == 0 && bt[1] == 0) continue;                                                \
+        T yr = cv[2 * c], yi = cv[2 * c + 1], v[2];                                            \
+        if (bt[0] == 1 && bt[1] == 0) { v[0] = yr; v[1] = yi; }                                \
+        else { v[0] = yr * bt[0] - yi * bt[1]; v[1] = yr * bt[1] + yi * bt[0]; }              \
+        CONV(fold, v, CI + ci * nb);                                                           \
+      }                                                                                        \
+    GEMM(fold, Order, TransA, TransB, M, N, K, alpha, A, lda, B, ldb, CI, ldci);               \
+    for (int i = 0; i < M; i++)                                                                \
+      for (int j = 0; j < N; j++) {                                                            \
+        size_t c = row ? (size_t)i * ldc + j : (size_t)j * ldc + i;                            \
+        size_t ci = row ? (size_t)i * ldci + j : (size_t)j * ldci + i;                         \
+        OUT(fold, CI + ci * nb, cv + 2 * c);                                                   \
+      }                                                                                        \
+    free(CI);                                                                                  \
+  }
+RBO_RXGEMM(rbo_rzgemm, double, rbo_zbzconv, rbo_zbzgemm, zconv)
+RBO_RXGEMM(rbo_rcgemm, float, rbo_cbcconv, rbo_cbcgemm, cconv)

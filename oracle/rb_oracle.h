@@ -115,6 +115,44 @@ void   rbo_rdgemm(int fold, char Order, char TransA, char TransB, int M, int N, 
                   double alpha, const double *A, int lda, const double *B, int ldb,
                   double beta, double *C, int ldc);
 
+/* ---- gemv / gemm of FP32 real and FP64 / FP32 complex elements ------------- */
+void   rbo_sbsconv(int fold, float x, float *Y);
+void   rbo_zbzconv(int fold, const double *x, double *Y);
+void   rbo_cbcconv(int fold, const float *x, float *Y);
+void   rbo_sbsgemv(int fold, char Order, char TransA, int M, int N, float alpha,
+                   const float *A, int lda, const float *X, int incX, float *Y, int incY);
+void   rbo_zbzgemv(int fold, char Order, char TransA, int M, int N, const void *alpha,
+                   const void *A, int lda, const void *X, int incX, double *Y, int incY);
+void   rbo_cbcgemv(int fold, char Order, char TransA, int M, int N, const void *alpha,
+                   const void *A, int lda, const void *X, int incX, float *Y, int incY);
+void   rbo_sbsgemm(int fold, char Order, char TransA, char TransB, int M, int N, int K,
+                   float alpha, const float *A, int lda, const float *B, int ldb, float *C,
+                   int ldc);
+void   rbo_zbzgemm(int fold, char Order, char TransA, char TransB, int M, int N, int K,
+                   const void *alpha, const void *A, int lda, const void *B, int ldb,
+                   double *C, int ldc);
+void   rbo_cbcgemm(int fold, char Order, char TransA, char TransB, int M, int N, int K,
+                   const void *alpha, const void *A, int lda, const void *B, int ldb,
+                   float *C, int ldc);
+void   rbo_rsgemv(int fold, char Order, char TransA, int M, int N, float alpha,
+                  const float *A, int lda, const float *X, int incX, float beta, float *Y,
+                  int incY);
+void   rbo_rzgemv(int fold, char Order, char TransA, int M, int N, const void *alpha,
+                  const void *A, int lda, const void *X, int incX, const void *beta, void *Y,
+                  int incY);
+void   rbo_rcgemv(int fold, char Order, char TransA, int M, int N, const void *alpha,
+                  const void *A, int lda, const void *X, int incX, const void *beta, void *Y,
+                  int incY);
+void   rbo_rsgemm(int fold, char Order, char TransA, char TransB, int M, int N, int K,
+                  float alpha, const float *A, int lda, const float *B, int ldb, float beta,
+                  float *C, int ldc);
+void   rbo_rzgemm(int fold, char Order, char TransA, char TransB, int M, int N, int K,
+                  const void *alpha, const void *A, int lda, const void *B, int ldb,
+                  const void *beta, void *C, int ldc);
+void   rbo_rcgemm(int fold, char Order, char TransA, char TransB, int M, int N, int K,
+                  const void *alpha, const void *A, int lda, const void *B, int ldb,
+                  const void *beta, void *C, int ldc);
+
 /* ---- exact reference for error statements (not ReproBLAS; see rb_oracle.c) */
 double rbo_exact_dot(int N, const double *X, int incX, const double *Y, int incY);
 

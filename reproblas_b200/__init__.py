@@ -120,6 +120,25 @@ SIGNATURES = {
                                  _c_vp]),
 }
 
+# gemv / gemm of FP32 real (scalars by value) and FP64 / FP32 complex elements (scalars by
+# pointer to two reals), same argument lists as the FP64 forms above
+for _t, _b, _sc in (("s", "sbs", _c_float), ("z", "zbz", _c_vp), ("c", "cbc", _c_vp)):
+    SIGNATURES["reproBLAS_r%sgemv" % _t] = (None, [_c_int, _c_char, _c_char, _c_int, _c_int, _sc, _c_vp,
+                                                    _c_int, _c_vp, _c_int, _sc, _c_vp, _c_int])
+    SIGNATURES["reproBLAS_%sgemv" % _t] = (None, [_c_char, _c_char, _c_int, _c_int, _sc, _c_vp, _c_int,
+                                                   _c_vp, _c_int, _sc, _c_vp, _c_int])
+    SIGNATURES["binnedBLAS_%sgemv" % _b] = (None, [_c_int, _c_char, _c_char, _c_int, _c_int, _sc, _c_vp,
+                                                    _c_int, _c_vp, _c_int, _c_vp, _c_int])
+    SIGNATURES["reproBLAS_r%sgemm" % _t] = (None, [_c_int, _c_char, _c_char, _c_char, _c_int, _c_int,
+                                                    _c_int, _sc, _c_vp, _c_int, _c_vp, _c_int, _sc,
+                                                    _c_vp, _c_int])
+    SIGNATURES["reproBLAS_%sgemm" % _t] = (None, [_c_char, _c_char, _c_char, _c_int, _c_int, _c_int,
+                                                   _sc, _c_vp, _c_int, _c_vp, _c_int, _sc, _c_vp,
+                                                   _c_int])
+    SIGNATURES["binnedBLAS_%sgemm" % _b] = (None, [_c_int, _c_char, _c_char, _c_char, _c_int, _c_int,
+                                                    _c_int, _sc, _c_vp, _c_int, _c_vp, _c_int, _c_vp,
+                                                    _c_int])
+
 class DgemmInstance(ctypes.Structure):
     """rb_dgemm_instance (include/reproblas_b200.h)"""
     _fields_ = [("order", ctypes.c_char), ("transa", ctypes.c_char), ("transb", ctypes.c_char),

@@ -31,32 +31,6 @@ const Blas23FoldOps* ops23(int fold) {
 bool is_row(char o) { return o == 'r' || o == 'R'; }
 bool is_nt(char t) { return t == 'n' || t == 'N'; }
 
-// Bump allocator over the workspace's big buffer (one call at a time holds the workspace).
-struct Bump {
-  unsigned char* base;
-  size_t off = 0;
-  void* take(size_t bytes) {
-    void* p = base + off;
-    off += (bytes + 255) / 256 * 256;
-    return p;
-  }
-};
-
-// Bytes spanned by `count` elements of `elem` bytes with stride `inc` elements.
-size_t span(long long count, long long inc, size_t elem) {
-  if (count <= 0) return 0;
-  return ((size_t)(count - 1) * (size_t)inc + 1) * elem;
-}
-
-// Make `p` (spanning `bytes`) available on the device: device pointers are used in place,
-// host ones are copied into the bump region.
-const void* to_device(const void* p, size_t bytes, Bump* b, cudaStream_t s, bool* ok) {
-  if (!p || bytes == 0 || on_device(p)) return p;
-  void* d = b->take(bytes);
-  if (!cuda_ok(cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, s), "copy operand")) *ok = false;
-  return d;
-}
-
 struct GemvReq {
   int fold;
   char order, trans;

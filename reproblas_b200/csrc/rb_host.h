@@ -90,4 +90,31 @@ int reduction_grid(long long work, int elems_per_thread, int threads, int occupa
 // Occupancy of the reduction kernels (CTAs per SM) for the chosen launch shape.
 int blas1_occupancy(char type, int fold, int op, bool vec, int threads);
 
+// ---- operand staging for the BLAS2/3 entry points ------------------------------------------
+// Bump allocator over the workspace's big buffer (one call at a time holds the workspace).
+struct Bump {
+  unsigned char* base;
+  size_t off = 0;
+  void* take(size_t bytes) {
+    void* p = base + off;
+    off += (bytes + 255) / 256 * 256;
+    return p;
+  }
+};
+
+// Bytes spanned by `count` elements of `elem` bytes with stride `inc` elements.
+inline size_t span(long long count, long long inc, size_t elem) {
+  if (count <= 0) return 0;
+  return ((size_t)(count - 1) * (size_t)inc + 1) * elem;
+}
+
+// Make `p` (spanning `bytes`) available on the device: device pointers are used in place,
+// host ones are copied into the bump region.
+inline const void* to_device(const void* p, size_t bytes, Bump* b, cudaStream_t s, bool* ok) {
+  if (!p || bytes == 0 || on_device(p)) return p;
+  void* d = b->take(bytes);
+  if (!cuda_ok(cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, s), "copy operand")) *ok = false;
+  return d;
+}
+
 }  // namespace rb

@@ -149,6 +149,54 @@ struct Blas23FoldOps {
 extern const Blas23FoldOps blas23_fold2, blas23_fold3, blas23_fold4, blas23_fold5,
     blas23_fold6, blas23_fold7, blas23_fold8;
 
+// ---- gemv / gemm for FP32 real, FP64 complex and FP32 complex elements (rb_xblas23_*.cu).
+// E is the real element type; complex operands are interleaved (re, im) pairs and every
+// stride / leading dimension counts whole (complex) elements.
+template <typename E>
+struct XGemvArgs {
+  long long R, C;             // rows kernel: R outputs x C reduction; cols kernel: C outputs x R
+  const E* A;
+  long long lda;
+  const E* x;
+  long long incx;
+  E ar, ai, br, bi;           // alpha, beta (imaginary parts 0 for real elements)
+  int alpha_one;              // skip the alpha multiply
+  int conj;                   // conjugate A's elements (complex ConjTrans)
+  int mode;                   // kOutValue / kOutBinned
+  int split;                  // rows kernel: warps per row (1, 2, 4, 8)
+  E* y;                       // kOutValue: values (stride incy)
+  E* ybin;                    // kOutBinned: binned states (stride incy states)
+  long long incy;
+  E* scratch;                 // cols kernel: partial states (gridDim.y > 1)
+  unsigned* tickets;          // cols kernel: one per column block, zero on entry
+};
+
+template <typename E>
+struct XGemmArgs {
+  long long M, N, K;
+  const E* A;
+  long long sai, sak;         // op(A)_ik = A[i*sai + k*sak]
+  const E* B;
+  long long sbk, sbj;         // op(B)_kj = B[k*sbk + j*sbj]
+  E ar, ai, br, bi;
+  int alpha_one;
+  int conja, conjb;           // conjugate op(A) / op(B) (complex ConjTrans)
+  int mode;
+  E* C;                       // kOutValue
+  E* Cbin;                    // kOutBinned
+  long long sci, scj;         // C_ij at offset i*sci + j*scj (values or states)
+};
+
+template <typename E>
+struct XOps {
+  cudaError_t (*gemv)(const XGemvArgs<E>& g, bool rows, dim3 grid, cudaStream_t s);
+  cudaError_t (*gemm)(const XGemmArgs<E>& g, cudaStream_t s);
+};
+// indexed by fold - 2 (folds 2..8)
+extern const XOps<float> xops_s[7];    // rb_xblas23_s.cu
+extern const XOps<double> xops_z[7];   // rb_xblas23_z.cu
+extern const XOps<float> xops_c[7];    // rb_xblas23_c.cu
+
 bool fold_supported(int fold);
 constexpr int kMaxFold = 8;
 

@@ -86,6 +86,20 @@ _SIGS = {
     "ssbconv": (c_float, [c_int, c_vp]),
 }
 
+# gemv / gemm of FP32 real (scalars by value) and complex (scalars by pointer) elements
+for _t, _b, _sc in (("s", "sbs", c_float), ("z", "zbz", c_vp), ("c", "cbc", c_vp)):
+    _SIGS[_b + "gemv"] = (None, [c_int, c_char, c_char, c_int, c_int, _sc, c_vp, c_int, c_vp,
+                                 c_int, c_vp, c_int])
+    _SIGS[_b + "gemm"] = (None, [c_int, c_char, c_char, c_char, c_int, c_int, c_int, _sc, c_vp,
+                                 c_int, c_vp, c_int, c_vp, c_int])
+    _SIGS["r" + _t + "gemv"] = (None, [c_int, c_char, c_char, c_int, c_int, _sc, c_vp, c_int, c_vp,
+                                       c_int, _sc, c_vp, c_int])
+    _SIGS["r" + _t + "gemm"] = (None, [c_int, c_char, c_char, c_char, c_int, c_int, c_int, _sc, c_vp,
+                                       c_int, c_vp, c_int, _sc, c_vp, c_int])
+_SIGS["sbsconv"] = (None, [c_int, c_float, c_vp])
+_SIGS["zbzconv"] = (None, [c_int, c_vp, c_vp])
+_SIGS["cbcconv"] = (None, [c_int, c_vp, c_vp])
+
 # reference-library names for the shared signatures
 _REF_NAMES = {
     "dbdsum": "binnedBLAS_dbdsum", "dbddot": "binnedBLAS_dbddot", "dbdssq": "binnedBLAS_dbdssq",
@@ -113,7 +127,13 @@ _REF_NAMES = {
     "dbdbaddsq": "binned_dbdbaddsq", "dbbound": "binned_dbbound", "dscale": "binned_dscale",
     "dindex": "binned_dindex", "sindex": "binned_sindex", "sbsbadd": "binned_sbsbadd",
     "ssbconv": "binned_ssbconv",
+    "sbsconv": "binned_sbsconv", "zbzconv": "binned_zbzconv", "cbcconv": "binned_cbcconv",
 }
+for _t, _b in (("s", "sbs"), ("z", "zbz"), ("c", "cbc")):
+    _REF_NAMES[_b + "gemv"] = "binnedBLAS_%sgemv" % _b
+    _REF_NAMES[_b + "gemm"] = "binnedBLAS_%sgemm" % _b
+    _REF_NAMES["r%sgemv" % _t] = "reproBLAS_r%sgemv" % _t
+    _REF_NAMES["r%sgemm" % _t] = "reproBLAS_r%sgemm" % _t
 
 
 class _Lib:

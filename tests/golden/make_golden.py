@@ -18,6 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
 from _ffi import ref, ptr, binned_zeros  # noqa: E402
 from _data import gen, gen_complex, blas23_operands  # noqa: E402
+from _data import XREAL, xblas23_cases, xblas23_case_operands, xscalar  # noqa: E402
 
 DISTS = ["uniform", "normal", "loguniform", "illcond", "sine", "bigsmall", "huge", "tiny"]
 NS = [1, 7, 1000, 4095, 20000]
@@ -180,13 +181,49 @@ def main():
                                "hash": h(np.concatenate([A, B, C])), "out": hexb(Co)})
                 seed += 1
 
+    # s / z / c gemv and gemm (xblas23_cases in tests/_data.py): the value form (r*gemv /
+    # r*gemm) and the binned form accumulating into empty states (stored as a hash).
+    xblas23 = []
+    for c in xblas23_cases():
+        t, fold = c["t"], c["fold"]
+        b = {"s": "sbs", "z": "zbz", "c": "cbc"}[t]
+        comps = 1 if t == "s" else 2
+        al, be = xscalar(t, complex(*c["alpha"])), xscalar(t, complex(*c["beta"]))
+        sa = al if t == "s" else ptr(al)
+        sb = be if t == "s" else ptr(be)
+        ops = xblas23_case_operands(c)
+        e = dict(c)
+        e["hash"] = h(np.concatenate([o.view(XREAL[t]) for o in ops]))
+        order, ta = c["order"].encode(), c["ta"].encode()
+        if c["kind"] == "gemv":
+            A, xv, yv = ops
+            yo = yv.copy()
+            getattr(R, "r%sgemv" % t)(fold, order, ta, c["M"], c["N"], sa, ptr(A), c["lda"],
+                                     ptr(xv), 1, sb, ptr(yo), 1)
+            zs = np.zeros(len(yv) * 2 * fold * comps, XREAL[t])
+            getattr(R, b + "gemv")(fold, order, ta, c["M"], c["N"], sa, ptr(A), c["lda"], ptr(xv),
+                                   1, ptr(zs), 1)
+        else:
+            A, B, C = ops
+            yo = C.copy()
+            tb = c["tb"].encode()
+            getattr(R, "r%sgemm" % t)(fold, order, ta, tb, c["M"], c["N"], c["K"], sa, ptr(A),
+                                     c["lda"], ptr(B), c["ldb"], sb, ptr(yo), c["ldc"])
+            zs = np.zeros(len(C) * 2 * fold * comps, XREAL[t])
+            getattr(R, b + "gemm")(fold, order, ta, tb, c["M"], c["N"], c["K"], sa, ptr(A),
+                                   c["lda"], ptr(B), c["ldb"], ptr(zs), c["ldc"])
+        e["out"] = hexb(yo)
+        e["states_hash"] = h(zs)
+        xblas23.append(e)
+
     out = {"generator": "tests/golden/make_golden.py", "reference": "ReproBLAS v2.1.0 "
            "compiled by oracle/Makefile (gcc -std=c99 -O3 -march=x86-64-v3)",
            "blas1": cases, "blas1_more": more, "dsum_config": cfg0, "special": special,
-           "blas23": blas23}
+           "blas23": blas23, "xblas23": xblas23}
     with open(os.path.join(HERE, "reference_golden.json"), "w") as f:
         json.dump(out, f, separators=(",", ":"))
-    print("wrote", len(cases), "blas1 cases,", len(special), "special,", len(blas23), "blas2/3")
+    print("wrote", len(cases), "blas1 cases,", len(special), "special,", len(blas23), "blas2/3,",
+          len(xblas23), "s/z/c blas2/3")
 
 
 if __name__ == "__main__":

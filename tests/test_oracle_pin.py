@@ -391,3 +391,148 @@ def test_port_matches_reference_amax(port):
             args = [n, ptr(a), inc] + ([ptr(b), inc] if b is not None else [])
             getattr(port, name)(*args, ptr(oa)); getattr(R, name)(*args, ptr(ob))
             assert same_value(oa, ob), (name, n, inc, dist)
+
+
+# ---- FP32 real / FP64 complex / FP32 complex gemv and gemm ---------------------------------
+from _data import XREAL, xblas23_case_operands, xscalar  # noqa: E402
+from _xblas import comps, lib_gemm, lib_gemv, real_view, reference_alpha_a, state_len  # noqa: E402
+
+
+def test_port_matches_golden_xblas23(port, golden):
+    bad = []
+    for c in golden["xblas23"]:
+        t, fold = c["t"], c["fold"]
+        ops = xblas23_case_operands(c)
+        assert _h(np.concatenate([real_view(t, o) for o in ops])) == c["hash"]
+        al, be = complex(*c["alpha"]), complex(*c["beta"])
+        if c["kind"] == "gemv":
+            A, xv, yv = ops
+            y = yv.copy()
+            lib_gemv(port, t, fold, c["order"], c["ta"], c["M"], c["N"], al, A, c["lda"], xv, 1, be, y, 1)
+            z = np.zeros(len(yv) * state_len(t, fold), XREAL[t])
+            lib_gemv(port, t, fold, c["order"], c["ta"], c["M"], c["N"], al, A, c["lda"], xv, 1, be, z, 1,
+                     binned=True)
+        else:
+            A, B, C = ops
+            y = C.copy()
+            lib_gemm(port, t, fold, c["order"], c["ta"], c["tb"], c["M"], c["N"], c["K"], al, A,
+                     c["lda"], B, c["ldb"], be, y, c["ldc"])
+            z = np.zeros(len(C) * state_len(t, fold), XREAL[t])
+            lib_gemm(port, t, fold, c["order"], c["ta"], c["tb"], c["M"], c["N"], c["K"], al, A,
+                     c["lda"], B, c["ldb"], be, z, c["ldc"], binned=True)
+        if not same_bits(real_view(t, y), from_hex(c["out"], XREAL[t])):
+            bad.append(("value", c["kind"], t, c["order"], c["ta"], c.get("tb")))
+        if _h(z) != c["states_hash"]:
+            bad.append(("states", c["kind"], t, c["order"], c["ta"], c.get("tb")))
+    assert not bad, bad
+
+
+def _xstates(L, t, fold, count, rng):
+    """`count` non-empty binned states of type t (binned(v) of normal values) from library L."""
+    n = state_len(t, fold)
+    z = np.zeros(count * n, XREAL[t])
+    for i in range(count):
+        if t == "s":
+            L.sbsconv(fold, float(np.float32(rng.standard_normal())), ptr(z[i * n:]))
+        else:
+            v = rng.standard_normal(2).astype(XREAL[t])
+            getattr(L, t + "b" + t + "conv")(fold, ptr(v), ptr(z[i * n:]))
+    return z
+
+
+def _xops(t, n, seed, dist):
+    if t == "s":
+        return gen(dist, n, seed, np.float32)
+    return gen_complex(dist, n, seed, np.complex128 if t == "z" else np.complex64)
+
+
+@needs_ref
+@pytest.mark.parametrize("t", ["s", "z", "c"])
+def test_port_matches_reference_live_xgemv(port, t):
+    """Every order and transpose, folds 2..8, strides, alpha / beta special values, value and
+    binned forms (into non-empty states). Float complex rows stay within 256 elements, where
+    the reference's cmcdotu state is the canonical one. Column-major conjugate transpose is
+    pinned on square shapes, and on M > N against the reference's truncated dot (its blocks
+    use N - j, zbzgemv.ccog:218: the first N elements of each column)."""
+    R = ref()
+    rng = np.random.default_rng(71 + ord(t))
+    for trial in range(72):
+        order, ta = "rc"[trial % 2], "ntc"[(trial // 2) % 3]
+        M, N = int(rng.integers(1, 180)), int(rng.integers(1, 180))
+        trunc = False
+        if order == "c" and ta == "c" and t != "s":
+            if trial % 4 == 1:
+                N = M
+            else:
+                M, N = max(M, N), min(M, N)   # M >= N: the reference reads N rows of A
+                trunc = M > N
+        fold = int(rng.integers(2, 9))
+        dist = ["uniform", "normal", "loguniform", "illcond"][trial % 4]
+        Rs, Cs = (M, N) if order == "r" else (N, M)
+        lda = Cs + int(rng.integers(0, 3))
+        A = _xops(t, Rs * lda, trial, dist)
+        lenx, leny = (N, M) if ta == "n" else (M, N)
+        incx, incy = int(rng.integers(1, 3)), int(rng.integers(1, 3))
+        X = _xops(t, lenx * incx, trial + 1, dist)
+        Y = _xops(t, leny * incy, trial + 2, "normal")
+        al = [1.0, 1.5 - 0.25j, 0.0, -2.0 + 0.5j][trial % 4]
+        be = [0.5 + 0.5j, 1.0, 0.0, -0.75][(trial // 4) % 4]
+        if t == "s":
+            al, be = complex(al).real, complex(be).real
+        Mp = N if trunc else M   # the oracle's view of the reference's computation
+        ya, yb = Y.copy(), Y.copy()
+        lib_gemv(port, t, fold, order, ta, Mp, N, al, A, lda, X, incx, be, ya, incy)
+        lib_gemv(R, t, fold, order, ta, M, N, al, A, lda, X, incx, be, yb, incy)
+        assert same_value(real_view(t, ya), real_view(t, yb)), (t, order, ta, M, N, fold, dist)
+        za = _xstates(port, t, fold, leny * incy, rng)
+        zb = za.copy()
+        lib_gemv(port, t, fold, order, ta, Mp, N, al, A, lda, X, incx, be, za, incy, binned=True)
+        lib_gemv(R, t, fold, order, ta, M, N, al, A, lda, X, incx, be, zb, incy, binned=True)
+        n = state_len(t, fold)
+        for i in range(leny * incy):
+            assert same_state(za[i * n:(i + 1) * n], zb[i * n:(i + 1) * n], fold, comps(t)), (t, order, ta, i)
+
+
+@needs_ref
+@pytest.mark.parametrize("t", ["s", "z", "c"])
+def test_port_matches_reference_live_xgemm(port, t):
+    """All 18 order / transpose combinations, folds 2..8, leading dimensions above the
+    minimum, alpha / beta special values, value and binned forms. For column-major complex
+    gemm with op(A) transposed and alpha != 1 the reference's A*alpha differs from the
+    mathematical product (reference_alpha_a); there the oracle is given the reference's
+    operands with alpha 1, which reproduces the reference's bits."""
+    R = ref()
+    rng = np.random.default_rng(170 + ord(t))
+    for trial in range(54):
+        order, ta, tb = "rc"[trial % 2], "ntc"[(trial // 2) % 3], "ntc"[(trial // 6) % 3]
+        M, N, K = int(rng.integers(1, 30)), int(rng.integers(1, 30)), int(rng.integers(1, 240))
+        fold = int(rng.integers(2, 9))
+        dist = ["uniform", "normal", "loguniform", "illcond"][trial % 4]
+        am, an = (M, K) if ta == "n" else (K, M)
+        bm, bn = (K, N) if tb == "n" else (N, K)
+        if order == "r":
+            lda, ldb, ldc = an + 1, bn, N + 2
+        else:
+            lda, ldb, ldc = am, bm + 1, M + 1
+        A = _xops(t, (am if order == "r" else an) * lda, trial, dist)
+        B = _xops(t, (bm if order == "r" else bn) * ldb, trial + 7, dist)
+        C = _xops(t, (M if order == "r" else N) * ldc, trial + 9, "normal")
+        al = [1.0, 1.5 - 0.25j, 0.0, -2.0 + 0.5j][(trial // 18) % 4 if trial % 3 else 1]
+        be = [0.5 + 0.5j, 1.0, 0.0, -0.75][trial % 4]
+        if t == "s":
+            al, be = complex(al).real, complex(be).real
+        Ap, alp = A, al
+        if t != "s" and order == "c" and ta != "n" and complex(al) not in (0, 1):
+            Ap, alp = reference_alpha_a(t, A, al, ta), 1.0
+        ca, cb = C.copy(), C.copy()
+        lib_gemm(port, t, fold, order, ta, tb, M, N, K, alp, Ap, lda, B, ldb, be, ca, ldc)
+        lib_gemm(R, t, fold, order, ta, tb, M, N, K, al, A, lda, B, ldb, be, cb, ldc)
+        assert same_value(real_view(t, ca), real_view(t, cb)), (t, order, ta, tb, M, N, K, fold)
+        nC = len(C)
+        za = _xstates(port, t, fold, nC, rng)
+        zb = za.copy()
+        lib_gemm(port, t, fold, order, ta, tb, M, N, K, alp, Ap, lda, B, ldb, be, za, ldc, binned=True)
+        lib_gemm(R, t, fold, order, ta, tb, M, N, K, al, A, lda, B, ldb, be, zb, ldc, binned=True)
+        n = state_len(t, fold)
+        for i in range(nC):
+            assert same_state(za[i * n:(i + 1) * n], zb[i * n:(i + 1) * n], fold, comps(t)), (t, order, ta, tb, i)
