@@ -54,7 +54,9 @@ def parse():
     p.add_argument("--no-secondary", action="store_true",
                    help="skip the dgemm (plain vs int8-sliced) and dgemv measurements")
     p.add_argument("--profile-kernel", choices=["int8", "plain_gemm", "gemv_n", "gemv_t", "zdotc",
-                                                "zsum", "csum", "dnrm2", "batched"],
+                                                "zsum", "csum", "dnrm2", "batched", "sgemv_n",
+                                                "sgemv_t", "zgemv_n", "zgemv_c", "cgemv_n",
+                                                "cgemv_c", "sgemm", "zgemm", "cgemm"],
                    help="only run that kernel `--steps` times on an n^3 (or n^2) case, for ncu")
     p.add_argument("--profile-n", type=int, default=2048)
     p.add_argument("--profile-m", type=int, default=0,
@@ -594,6 +596,48 @@ def secondary(args):
                 "frac_of_copy_peak": round(byts / t / 1e9 / peaks()[0], 3)}
             del x, y
         del A
+    out.update(xblas23_cases(torch, rb, rng))
+    return out
+
+
+def xblas23_cases(torch, rb, rng):
+    """FP32 real / FP64 complex / FP32 complex gemv (NoTrans and ConjTrans, 128 MiB and 1 GiB
+    matrices) and gemm (M = N = K = 1024), row-major, fold 3, alpha 1.5 (complex 1.5 - 0.25i),
+    beta 0.5, device-resident operands. gemv bytes: A + x + y read + y written; gemm work in
+    real flops (complex: 8 per multiply-add) and binned deposits (complex: 4 per multiply-add)."""
+    out = {}
+    real = {"s": np.float32, "z": np.float64, "c": np.float32}
+    shapes = {"s": ((8192, 4096), (16384, 16384)), "z": ((4096, 2048), (8192, 8192)),
+              "c": ((4096, 4096), (8192, 16384))}
+    for t in "szc":
+        nc = 1 if t == "s" else 2
+        es = np.dtype(real[t]).itemsize * nc
+        al = 1.5 if t == "s" else np.array([1.5, -0.25], real[t])
+        be = 0.5 if t == "s" else np.array([0.5, 0.0], real[t])
+        for (m, n) in shapes[t]:
+            A = torch.from_numpy(rng.uniform(-1, 1, m * n * nc).astype(real[t])).cuda()
+            for ta in ("n", "c" if t != "s" else "t"):
+                lx, ly = (n, m) if ta == "n" else (m, n)
+                x = torch.from_numpy(rng.uniform(-1, 1, lx * nc).astype(real[t])).cuda()
+                y = torch.from_numpy(rng.uniform(-1, 1, ly * nc).astype(real[t])).cuda()
+                call = lambda: rb.call("reproBLAS_r%sgemv" % t, 3, "r", ta, m, n, al, A, n, x, 1, be, y, 1)
+                t_s = _event_time(torch, call, 5 if m * n * es > 2 ** 28 else 20, warm=3)
+                byts = float(es) * (m * n + lx + 2 * ly)
+                out["%sgemv_%dx%d_%s" % (t, m, n, ta)] = {
+                    "gbs": round(byts / t_s / 1e9, 1), "us": round(t_s * 1e6, 2),
+                    "frac_of_copy_peak": round(byts / t_s / 1e9 / peaks()[0], 3)}
+                del x, y
+            del A
+        k = 1024
+        A = torch.from_numpy(rng.uniform(-1, 1, k * k * nc).astype(real[t])).cuda()
+        B = torch.from_numpy(rng.uniform(-1, 1, k * k * nc).astype(real[t])).cuda()
+        C = torch.from_numpy(rng.uniform(-1, 1, k * k * nc).astype(real[t])).cuda()
+        t_s = _event_time(torch, lambda: rb.call("reproBLAS_r%sgemm" % t, 3, "r", "n", "n", k, k, k, al, A, k,
+                                                 B, k, be, C, k), 3, warm=1)
+        flops = (2.0 if t == "s" else 8.0) * k ** 3
+        out["%sgemm_1024" % t] = {"gflops": round(flops / t_s / 1e9, 1), "ms": round(t_s * 1e3, 3),
+                                  "gdeposits_per_s": round(k ** 3 * nc * nc / t_s / 1e9, 1)}
+        del A, B, C
     return out
 
 
@@ -611,6 +655,29 @@ def profile_case(args):
         y = torch.from_numpy(rng.uniform(-1, 1, m if ta == "n" else n)).cuda()
         for _ in range(args.warmup + args.steps):
             rb.call("reproBLAS_rdgemv", 3, "r", ta, m, n, 1.5, A, n, x, 1, 0.5, y, 1)
+        torch.cuda.synchronize()
+        print("profile case done: %s m=%d n=%d" % (args.profile_kernel, m, n))
+        return
+    if args.profile_kernel[0] in "szc" and args.profile_kernel[1:4] == "gem":
+        # FP32 real / complex gemv (m x n, row-major) or gemm (n^3), fold 3, uniform(-1, 1)
+        t, kind = args.profile_kernel[0], args.profile_kernel[1:5]
+        nc = 1 if t == "s" else 2
+        real = np.float64 if t == "z" else np.float32
+        al = 1.5 if t == "s" else np.array([1.5, -0.25], real)
+        be = 0.5 if t == "s" else np.array([0.5, 0.0], real)
+        m = args.profile_m or n
+        if kind == "gemv":
+            ta = args.profile_kernel[-1]
+            A = torch.from_numpy(rng.uniform(-1, 1, m * n * nc).astype(real)).cuda()
+            x = torch.from_numpy(rng.uniform(-1, 1, (n if ta == "n" else m) * nc).astype(real)).cuda()
+            y = torch.from_numpy(rng.uniform(-1, 1, (m if ta == "n" else n) * nc).astype(real)).cuda()
+            for _ in range(args.warmup + args.steps):
+                rb.call("reproBLAS_r%sgemv" % t, 3, "r", ta, m, n, al, A, n, x, 1, be, y, 1)
+        else:
+            A, B, C = (torch.from_numpy(rng.uniform(-1, 1, n * n * nc).astype(real)).cuda()
+                       for _ in range(3))
+            for _ in range(args.warmup + args.steps):
+                rb.call("reproBLAS_r%sgemm" % t, 3, "r", "n", "n", n, n, n, al, A, n, B, n, be, C, n)
         torch.cuda.synchronize()
         print("profile case done: %s m=%d n=%d" % (args.profile_kernel, m, n))
         return
