@@ -454,6 +454,22 @@ unsigned long long rb_kernel_launch_count(void);
 int rb_dbdbadd_states(const int fold, const int count, const double_binned *states,
                       double_binned *out);
 
+/* The same for the other state kinds, one per binnedMPI operation: float_binned
+ * (src/binnedMPI/SBSBADD.ccog, binned_sbsbadd), double_complex_binned (ZBZBADD.ccog,
+ * binned_zbzbadd) and float_complex_binned (CBCBADD.ccog, binned_cbcbadd) states; and the
+ * scaled sum-of-squares records [scale, binned state] of the 2-norms (DBDBADDSQ.ccog:9-14 /
+ * SBSBADDSQ.ccog, binned_dbdbaddsq / sbsbaddsq; 1 + 2*fold elements each), where `out`'s
+ * scale is updated too. Device memory, enqueued on the current stream; any order gives the
+ * same bits. Return an RB_* code. */
+int rb_sbsbadd_states(const int fold, const int count, const float_binned *states,
+                      float_binned *out);
+int rb_zbzbadd_states(const int fold, const int count, const double_complex_binned *states,
+                      double_complex_binned *out);
+int rb_cbcbadd_states(const int fold, const int count, const float_complex_binned *states,
+                      float_complex_binned *out);
+int rb_dbdbaddsq_states(const int fold, const int count, const double *states, double *out);
+int rb_sbsbaddsq_states(const int fold, const int count, const float *states, float *out);
+
 /* Reproducible dot product that allocates nothing. No counterpart in the reference.
  * For callers that may not allocate device memory where they need the dot product:
  * plugins whose host application owns the whole device-memory budget, and

@@ -1899,3 +1899,23 @@ RBO_RXGEMV(rbo_rcgemv, float, rbo_cbcconv, rbo_cbcgemv, cconv)
   }
 RBO_RXGEMM(rbo_rzgemm, double, rbo_zbzconv, rbo_zbzgemm, zconv)
 RBO_RXGEMM(rbo_rcgemm, float, rbo_cbcconv, rbo_cbcgemm, cconv)
+
+/* ------------------------------------------------------------------------- */
+/* State merges of the remaining kinds (the binnedMPI operations)              */
+/* ------------------------------------------------------------------------- */
+/* src/binned/zbzbadd.c -> zmzmadd.c: each component through dmdmadd, stride 2 */
+void rbo_zbzbadd(int fold, const double *X, double *Y) {
+  for (int c = 0; c < 2; c++)
+    rbo_dmdmadd(fold, X + c, 2, X + 2 * fold + c, 2, Y + c, 2, Y + 2 * fold + c, 2);
+}
+
+/* src/binned/cbcbadd.c -> cmcmadd.c */
+void rbo_cbcbadd(int fold, const float *X, float *Y) {
+  for (int c = 0; c < 2; c++)
+    rbo_smsmadd(fold, X + c, 2, X + 2 * fold + c, 2, Y + c, 2, Y + 2 * fold + c, 2);
+}
+
+/* src/binned/sbsbaddsq.c -> smsmaddsq.c */
+float rbo_sbsbaddsq(int fold, float scaleX, const float *X, float scaleY, float *Y) {
+  return smsmaddsq(fold, scaleX, X, 1, X + fold, 1, scaleY, Y, 1, Y + fold, 1);
+}

@@ -153,6 +153,10 @@ void   rbo_rcgemm(int fold, char Order, char TransA, char TransB, int M, int N, 
                   const void *alpha, const void *A, int lda, const void *B, int ldb,
                   const void *beta, void *C, int ldc);
 
+void   rbo_zbzbadd(int fold, const double *X, double *Y);
+void   rbo_cbcbadd(int fold, const float *X, float *Y);
+float  rbo_sbsbaddsq(int fold, float scaleX, const float *X, float scaleY, float *Y);
+
 /* ---- exact reference for error statements (not ReproBLAS; see rb_oracle.c) */
 double rbo_exact_dot(int N, const double *X, int incX, const double *Y, int incY);
 

@@ -116,6 +116,11 @@ SIGNATURES = {
     "rb_kernel_launch_count": (ctypes.c_ulonglong, []),
     "rb_version": (ctypes.c_char_p, []),
     "rb_dbdbadd_states": (_c_int, [_c_int, _c_int, _c_vp, _c_vp]),
+    "rb_sbsbadd_states": (_c_int, [_c_int, _c_int, _c_vp, _c_vp]),
+    "rb_zbzbadd_states": (_c_int, [_c_int, _c_int, _c_vp, _c_vp]),
+    "rb_cbcbadd_states": (_c_int, [_c_int, _c_int, _c_vp, _c_vp]),
+    "rb_dbdbaddsq_states": (_c_int, [_c_int, _c_int, _c_vp, _c_vp]),
+    "rb_sbsbaddsq_states": (_c_int, [_c_int, _c_int, _c_vp, _c_vp]),
     "rb_ddot_noalloc": (_c_int, [_c_int, _c_int, _c_vp, _c_int, _c_vp, _c_int, _c_vp, _c_vp,
                                  _c_vp]),
 }

@@ -98,27 +98,64 @@ bool run_xgemv(const XGemvReq<E, CX>& q) {
   const size_t x_bytes = span(nred_eff, q.incX, es);
   const size_t y_bytes = q.mode == kOutValue ? span(nout, q.incY, es)
                                              : ((size_t)(nout - 1) * q.incY + 1) * per_state;
-  // cols kernel: column blocks of 256 outputs, row chunks to fill about 8 CTAs per SM, each
-  // chunk at least 64 rows, at most 256 chunks (the last CTA merges them serially)
+  // 16-byte loads when every row of A starts 16-byte aligned (host operands are staged to
+  // aligned device memory)
+  const bool a_vec = (!on_device(q.A) || ((uintptr_t)q.A % 16) == 0) && ((size_t)q.lda * es) % 16 == 0;
+  // cols kernel shape: G row groups per CTA of T = 256/G threads, W columns per thread (one
+  // 16-byte vector), column blocks of T*W outputs, row chunks. Cost model in units of one row
+  // per thread: the streaming part (waves of CTAs times rows per thread, plus the in-CTA
+  // tree merge) and the serial merge of the chunk partials in the last CTA of each column
+  // block (about 4 units per merge).
   long long col_blocks = 0, nchunks = 1;
+  int groups = 1;
   size_t part_bytes = 0;
-  if (!nt) {
-    col_blocks = (nout + 255) / 256;
-    const long long target = (long long)di.sms * 8;
-    nchunks = (target + col_blocks - 1) / col_blocks;
-    const long long maxch = (nred_eff + 63) / 64;
-    if (nchunks > maxch) nchunks = maxch;
-    if (nchunks > 256) nchunks = 256;
-    if (nchunks < 1) nchunks = 1;
+  long long rows_grid = 1;
+  if (nt) {
+    // rows kernel: the R*C products split evenly over up to 8 CTAs (of 8 warps) per SM, at
+    // least 1024 products per warp; two scratch records per warp for the rows it cuts
+    const long long total = nout * nred_eff;
+    rows_grid = (total + 8 * 1024 - 1) / (8 * 1024);
+    if (rows_grid > (long long)di.sms * 8) rows_grid = (long long)di.sms * 8;
+    if (rows_grid < 1) rows_grid = 1;
+    part_bytes = (size_t)rows_grid * 8 * 2 * NC * (2 * q.fold + 1) * sizeof(E);
+    if (!w->ensure_tickets((size_t)nout)) return false;
+  } else {
+    const long long W = (long long)(16 / es);
+    // resident CTAs: the kernels are built for 3 per SM up to fold 3, 2 above
+    const long long slots = (long long)di.sms * (q.fold <= 3 ? 3 : 2);
+    long long best = -1;
+    for (int G = 1; G <= 8; G *= 2) {
+      const long long cols = (256 / G) * W;
+      const long long cb = (nout + cols - 1) / cols;
+      const long long maxch = (nred_eff + 8 * G - 1) / (8 * G);   // >= 8 rows per group
+      const long long lg = G == 1 ? 0 : G == 2 ? 1 : G == 4 ? 2 : 3;
+      for (long long ch : {slots / cb, (slots + cb - 1) / cb}) {
+        if (ch > maxch) ch = maxch;
+        if (ch > 1024) ch = 1024;
+        if (ch < 1) ch = 1;
+        const long long rpt = ((nred_eff + ch - 1) / ch + G - 1) / G;
+        const long long waves = (cb * ch + slots - 1) / slots;
+        const long long cost = waves * (rpt + 8 * lg) + 4 * ((ch + G - 1) / G + 2 * lg);
+        if (best < 0 || cost < best) {
+          best = cost;
+          groups = G;
+          col_blocks = cb;
+          nchunks = ch;
+        }
+      }
+    }
     if (nchunks > 1) {
       part_bytes = (size_t)nchunks * nout * NC * (2 * q.fold + 1) * sizeof(E);
       if (!w->ensure_tickets((size_t)col_blocks)) return false;
     }
   }
+  // fl(alpha*x) in a contiguous aligned buffer: the rows kernel's 16-byte loads, and one
+  // multiply per row instead of one per row and thread in the cols kernel
+  const size_t bx_bytes = nred_eff > 0 ? (size_t)nred_eff * es : 0;
   const bool a_host = a_bytes && !on_device(q.A), x_host = x_bytes && !on_device(q.X);
   const bool y_host = !on_device(q.Y);
-  const size_t need = part_bytes + (a_host ? a_bytes : 0) + (x_host ? x_bytes : 0) +
-                      (y_host ? y_bytes : 0) + 4 * 256;
+  const size_t need = part_bytes + bx_bytes + (a_host ? a_bytes : 0) + (x_host ? x_bytes : 0) +
+                      (y_host ? y_bytes : 0) + 5 * 256;
   if (!w->ensure_big(need)) return false;
   Bump b{w->big};
   bool ok = true;
@@ -126,6 +163,7 @@ bool run_xgemv(const XGemvReq<E, CX>& q) {
   const E* dX = (const E*)to_device(q.X, x_bytes, &b, s, &ok);
   E* dY = (E*)to_device(q.Y, y_bytes, &b, s, &ok);
   E* part = part_bytes ? (E*)b.take(part_bytes) : nullptr;
+  E* bx = bx_bytes ? (E*)b.take(bx_bytes) : nullptr;
   if (!ok) return false;
 
   XGemvArgs<E> g{};
@@ -145,19 +183,29 @@ bool run_xgemv(const XGemvReq<E, CX>& q) {
   g.incy = q.incY;
   count_launch();
   cudaError_t e;
+  if (nred_eff > 0 && !(g.alpha_one && q.incX == 1 && ((uintptr_t)dX % 16) == 0)) {
+    long long sg = (nred_eff + 255) / 256;
+    if (sg > (long long)di.sms * 4) sg = (long long)di.sms * 4;
+    count_launch();
+    if (!cuda_ok(o->scale_x(dX, nred_eff, q.incX, g.ar, g.ai, g.alpha_one, bx, (int)sg, s),
+                 "gemv scale launch"))
+      return false;
+    g.x = bx;
+    g.incx = 1;
+    g.alpha_one = 1;
+  }
+  g.vec = a_vec && ((uintptr_t)dA % 16) == 0 ? 1 : 0;
   if (nt) {
     g.R = nout;
     g.C = nred_eff;
-    const long long target_warps = (long long)di.sms * 16;
-    int S = 1;
-    while (S < 8 && nout * S < target_warps) S *= 2;
-    g.split = S;
-    const int rows_per_cta = 8 / S;
-    e = o->gemv(g, true, dim3((unsigned)((nout + rows_per_cta - 1) / rows_per_cta)), s);
+    g.split = 1;
+    g.scratch = part;
+    g.tickets = w->tickets;
+    e = o->gemv(g, true, dim3((unsigned)rows_grid), s);   // clamped to the resident grid
   } else {
     g.C = nout;
     g.R = nred_eff;
-    g.split = 1;
+    g.split = groups;
     g.scratch = part;
     g.tickets = w->tickets;
     e = o->gemv(g, false, dim3((unsigned)col_blocks, (unsigned)nchunks), s);

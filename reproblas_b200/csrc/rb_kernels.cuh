@@ -163,12 +163,15 @@ struct XGemvArgs {
   int alpha_one;              // skip the alpha multiply
   int conj;                   // conjugate A's elements (complex ConjTrans)
   int mode;                   // kOutValue / kOutBinned
-  int split;                  // rows kernel: warps per row (1, 2, 4, 8)
+  int split;                  // cols kernel: row groups per CTA (1, 2, 4, 8)
+  int vec;                    // rows kernel: 16-byte loads (rows and x aligned, incx 1, x
+                              // already multiplied by alpha)
   E* y;                       // kOutValue: values (stride incy)
   E* ybin;                    // kOutBinned: binned states (stride incy states)
   long long incy;
-  E* scratch;                 // cols kernel: partial states (gridDim.y > 1)
-  unsigned* tickets;          // cols kernel: one per column block, zero on entry
+  E* scratch;                 // partial states: rows kernel 2 per warp, cols kernel per chunk
+  unsigned* tickets;          // rows kernel: one per row; cols kernel: one per column block;
+                              // zero on entry, zero again on exit
 };
 
 template <typename E>
@@ -191,6 +194,9 @@ template <typename E>
 struct XOps {
   cudaError_t (*gemv)(const XGemvArgs<E>& g, bool rows, dim3 grid, cudaStream_t s);
   cudaError_t (*gemm)(const XGemmArgs<E>& g, cudaStream_t s);
+  // bx_i = fl(alpha * x_i) for i < n, contiguous (the rows kernel's vector input)
+  cudaError_t (*scale_x)(const E* x, long long n, long long incx, E ar, E ai, int alpha_one,
+                         E* bx, int grid, cudaStream_t s);
 };
 // indexed by fold - 2 (folds 2..8)
 extern const XOps<float> xops_s[7];    // rb_xblas23_s.cu

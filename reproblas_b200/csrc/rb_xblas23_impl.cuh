@@ -165,31 +165,155 @@ __device__ __forceinline__ void merge_rec(Acc<E, F>& a, const E* rec, long long 
   a.merge(o);
 }
 
+// 16-byte read-only load of 16 / sizeof(E) reals (the address is 16-byte aligned).
+template <typename E>
+__device__ __forceinline__ void ld16(const E* p, E (&v)[16 / sizeof(E)]) {
+  if constexpr (sizeof(E) == 8) {
+    const double2 t = __ldg((const double2*)p);
+    v[0] = t.x;
+    v[1] = t.y;
+  } else {
+    const float4 t = __ldg((const float4*)p);
+    v[0] = t.x;
+    v[1] = t.y;
+    v[2] = t.z;
+    v[3] = t.w;
+  }
+}
+
+// Deposit one tile into the NC accumulators of an entry: complex entries interleave their
+// real and imaginary chains (tile2); every one of the KD values counts toward the endurance.
+template <typename E, bool CX, int F, int KD>
+__device__ __forceinline__ void deposit_tile(Acc<E, F> (&a)[CX ? 2 : 1], const E (&v)[CX ? 2 : 1][KD],
+                                             int nv) {
+  if constexpr (CX) tile2<E, F, KD>(a[0], v[0], a[1], v[1]);
+  else a[0].template tile<KD>(v[0], nv);
+}
+
 // ---------------------------------------------------------------------------------------
-// gemv, reduction along contiguous rows: out_r = sum_c op(A[r*lda + c]) * fl(alpha*x_c).
-// S warps share a row (S = 1, 2, 4, 8); a CTA of 8 warps covers 8/S rows; lanes stride the
-// row so a warp reads 32 consecutive elements per step.
+// gemv, reduction along contiguous rows: out_r = sum_c op(A[r*lda + c]) * bx_c, with
+// bx = fl(alpha*x). The R*C products, in row-major order, are split evenly over all warps of
+// a resident grid (boundaries rounded down to whole 16-byte vectors of a row), so each warp
+// streams the same amount of A and cuts at most its first and its last row. A row a warp
+// holds whole is reduced over the warp and finished by it; a cut row's part goes to scratch
+// slot 2w (the warp's first row) or 2w+1 (its last row) with the row's arrival ticket, and
+// the warp that completes the row merges its parts (lanes take the parts, then a butterfly)
+// and finishes it. With g.vec (row starts and x 16-byte aligned, incx 1, x already multiplied
+// by alpha) a lane reads NV 16-byte vectors of the row and of x per tile -- 32 consecutive
+// vectors per warp load; ragged row ends go through the element path. No CTA-wide
+// synchronisation. Warps beyond one per 1024 products stay idle, so no range is empty.
 // ---------------------------------------------------------------------------------------
+template <typename E, bool CX>
+struct RowsCfg {
+  static constexpr int NC = CX ? 2 : 1, D = CX ? 2 : 1;
+  static constexpr int PER = 16 / (int)sizeof(E);   // reals per 16-byte vector
+  static constexpr int VE = PER / NC;               // elements per vector: z 1, c 2, s 4
+  static constexpr int NV = CX ? 2 : 4;             // vectors per lane per tile
+  static constexpr int KE = NV * VE;                // elements per lane per tile
+  static constexpr int KD = KE * D;                 // deposits per component per tile
+};
+
+// Even split of `total` row-major elements of rows of C over nw warps: warp w starts at
+// floor(w*total/nw), rounded down to a multiple of VE within its row.
+struct RowSplit {
+  long long total, C, q, rem;
+  int nw, ve;
+  __device__ __forceinline__ RowSplit(long long total_, long long C_, int nw_, int ve_)
+      : total(total_), C(C_), nw(nw_), ve(ve_) {
+    q = total / nw;
+    rem = total - q * nw;
+  }
+  __device__ __forceinline__ long long start(long long w) const {
+    if (w >= nw) return total;
+    const long long b = w * q + (w * rem) / nw;   // floor(w * total / nw) without overflow
+    const long long r = b / C;
+    const long long c = b - r * C;
+    return r * C + (c - c % ve);
+  }
+  // the warp whose range holds element e (0 <= e < total)
+  __device__ __forceinline__ long long owner(long long e) const {
+    long long w = (long long)((double)e * (double)nw / (double)total);
+    if (w >= nw) w = nw - 1;
+    if (w < 0) w = 0;
+    for (int i = 0; i < 64 && w + 1 < nw && start(w + 1) <= e; i++) w++;
+    for (int i = 0; i < 64 && w > 0 && start(w) > e; i++) w--;
+    return w;
+  }
+};
+
 template <typename E, bool CX, int F>
-__global__ void __launch_bounds__(256) xgemv_rows_kernel(XGemvArgs<E> g) {
-  constexpr int NC = CX ? 2 : 1, D = CX ? 2 : 1, K = 4;
+__global__ void __launch_bounds__(256, F <= 3 ? 3 : 2) xgemv_rows_kernel(XGemvArgs<E> g) {
+  using Cfg = RowsCfg<E, CX>;
+  constexpr int NC = Cfg::NC, D = Cfg::D, PER = Cfg::PER, VE = Cfg::VE, NV = Cfg::NV;
+  constexpr int KD = Cfg::KD, K = 4;
   constexpr int REC = NC * (2 * F + 1);
-  __shared__ E smem[8 * REC];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int S = g.split;
-  const int rows_per_cta = 8 / S;
-  const int rloc = warp / S, part = warp % S;
-  const long long r = (long long)blockIdx.x * rows_per_cta + rloc;
-  Acc<E, F> a[NC];
-#pragma unroll
-  for (int c = 0; c < NC; c++) a[c].zero();
-  if (r < g.R) {
-    const E* row = g.A + r * g.lda * NC;
-    const long long chunk = (g.C + S - 1) / S;
-    const long long c0 = part * chunk < g.C ? part * chunk : g.C;
-    const long long c1 = c0 + chunk < g.C ? c0 + chunk : g.C;
+  const int lane = threadIdx.x & 31;
+  const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (int)(((long long)gridDim.x * blockDim.x) >> 5);
+  if (g.C == 0) {
+    // no products (alpha == 0): every entry is its initial state
 #pragma unroll 1
-    for (long long b = c0 + lane; b < c1; b += 32 * K) {
+    for (long long r = gwarp; r < g.R; r += nw) {
+      Acc<E, F> a[NC];
+#pragma unroll
+      for (int q = 0; q < NC; q++) a[q].zero();
+      if (lane == 0)
+        finish<E, CX, F>(a, g.mode, g.y + r * g.incy * NC, g.br, g.bi, g.ybin + r * g.incy * 2 * F * NC);
+    }
+    return;
+  }
+  // warps in the split: at least 1024 elements each (so every range is non-empty)
+  long long nwe = g.R * g.C / 1024;
+  nwe = nwe < 1 ? 1 : nwe > nw ? nw : nwe;
+  if (gwarp >= nwe) return;
+  const RowSplit sp(g.R * g.C, g.C, (int)nwe, VE);
+  const long long b0 = sp.start(gwarp), b1 = sp.start(gwarp + 1);
+#pragma unroll 1
+  for (long long pos = b0; pos < b1;) {
+    const long long r = pos / g.C;
+    const long long c0 = pos - r * g.C;
+    const long long c1 = (r + 1) * g.C <= b1 ? g.C : b1 - r * g.C;
+    Acc<E, F> a[NC];
+#pragma unroll
+    for (int q = 0; q < NC; q++) a[q].zero();
+    const E* row = g.A + r * g.lda * NC;
+    long long ce = c0;   // start of the element path
+    if (g.vec) {
+      const long long nvec = (c1 - c0) / VE;
+#pragma unroll 1
+      for (long long vb = lane; vb < nvec; vb += 32 * NV) {
+        E v[NC][KD];
+#pragma unroll
+        for (int q = 0; q < NC; q++)
+#pragma unroll
+          for (int d = 0; d < KD; d++) v[q][d] = E(0);
+        int nv = 0;
+#pragma unroll
+        for (int j = 0; j < NV; j++) {
+          const long long vi = vb + 32 * j;
+          if (vi < nvec) {
+            E av[PER], xv[PER];
+            ld16<E>(row + (c0 + vi * VE) * NC, av);
+            ld16<E>(g.x + (c0 + vi * VE) * NC, xv);
+#pragma unroll
+            for (int e = 0; e < VE; e++) {
+              Val<E, CX> aa, xx;
+              aa.r = av[e * NC];
+              xx.r = xv[e * NC];
+              aa.i = CX ? av[e * NC + NC - 1] : E(0);
+              xx.i = CX ? xv[e * NC + NC - 1] : E(0);
+              if (CX && g.conj) aa.i = -aa.i;
+              products<E, CX, KD>(aa, xx, v, j * VE + e);
+            }
+            nv = (j + 1) * VE * D;
+          }
+        }
+        deposit_tile<E, CX, F, KD>(a, v, nv);
+      }
+      ce = c0 + nvec * VE;
+    }
+#pragma unroll 1
+    for (long long b = ce + lane; b < c1; b += 32 * K) {
       E v[NC][K * D];
       int nv = 0;
 #pragma unroll
@@ -205,98 +329,201 @@ __global__ void __launch_bounds__(256) xgemv_rows_kernel(XGemvArgs<E> g) {
           Val<E, CX> xv = ldv<E, CX>(g.x, c * g.incx);
           if (!g.alpha_one) xv = scale<E, CX>(xv, g.ar, g.ai);
           products<E, CX, K * D>(av, xv, v, k);
-          nv = k + 1;
+          nv = (k + 1) * D;
         }
       }
-#pragma unroll
-      for (int q = 0; q < NC; q++) a[q].template tile<K * D>(v[q], nv * D);
+      deposit_tile<E, CX, F, K * D>(a, v, nv);
     }
-  }
 #pragma unroll
-  for (int q = 0; q < NC; q++) {
-    a[q].renorm();
+    for (int q = 0; q < NC; q++) {
+      a[q].renorm();
 #pragma unroll 1
-    for (int m = 16; m; m >>= 1) a[q].merge(a[q].shfl_xor(m));
-  }
-  if (lane == 0) {
-#pragma unroll
-    for (int q = 0; q < NC; q++) put_rec<E, F>(a[q], smem + warp * REC + q * (2 * F + 1), 1);
-  }
-  __syncthreads();
-  if (threadIdx.x < rows_per_cta) {
-    const long long rr = (long long)blockIdx.x * rows_per_cta + threadIdx.x;
-    if (rr < g.R) {
-      Acc<E, F> t[NC];
-#pragma unroll
-      for (int q = 0; q < NC; q++) {
-        t[q].zero();
-        for (int p = 0; p < S; p++)
-          merge_rec<E, F, false>(t[q], smem + (threadIdx.x * S + p) * REC + q * (2 * F + 1), 1);
-      }
-      finish<E, CX, F>(t, g.mode, g.y + rr * g.incy * NC, g.br, g.bi,
-                       g.ybin + rr * g.incy * 2 * F * NC);
+      for (int m = 16; m; m >>= 1) a[q].merge(a[q].shfl_xor(m));
     }
+    bool done = c0 == 0 && c1 == g.C;   // the whole row is this warp's
+    if (!done) {
+      const long long slot = pos == b0 ? 2 * gwarp : 2 * gwarp + 1;
+      unsigned tk = 0;
+      if (lane == 0) {
+        E* rec = g.scratch + slot * REC;
+#pragma unroll
+        for (int q = 0; q < NC; q++) put_rec<E, F>(a[q], rec + q * (2 * F + 1), 1);
+        __threadfence();
+        tk = atomicAdd(g.tickets + r, 1u);
+      }
+      tk = __shfl_sync(0xffffffffu, tk, 0);
+      const long long fw = sp.owner(r * g.C), lw = sp.owner(r * g.C + g.C - 1);
+      if ((long long)tk == lw - fw) {
+        __threadfence();
+        // lanes take the parts of warps fw + lane, fw + lane + 32, ...; then a butterfly
+#pragma unroll
+        for (int q = 0; q < NC; q++) a[q].zero();
+#pragma unroll 1
+        for (long long v = fw + lane; v <= lw; v += 32) {
+          const long long vs = sp.start(v) / g.C == r ? 2 * v : 2 * v + 1;
+#pragma unroll
+          for (int q = 0; q < NC; q++)
+            merge_rec<E, F, true>(a[q], g.scratch + vs * REC + q * (2 * F + 1), 1);
+        }
+#pragma unroll
+        for (int q = 0; q < NC; q++) {
+#pragma unroll 1
+          for (int m = 16; m; m >>= 1) a[q].merge(a[q].shfl_xor(m));
+        }
+        if (lane == 0) g.tickets[r] = 0u;
+        done = true;
+      }
+    }
+    if (done && lane == 0)
+      finish<E, CX, F>(a, g.mode, g.y + r * g.incy * NC, g.br, g.bi, g.ybin + r * g.incy * 2 * F * NC);
+    pos = (r + 1) * g.C;
+  }
+}
+
+// fl(alpha * x_i) for i < n into a contiguous buffer (the x of the vectorised rows kernel).
+template <typename E, bool CX>
+__global__ void __launch_bounds__(256) xscale_kernel(const E* x, long long n, long long incx, E ar,
+                                                     E ai, int alpha_one, E* bx) {
+  constexpr int NC = CX ? 2 : 1;
+  const long long step = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += step) {
+    Val<E, CX> v = ldv<E, CX>(x, i * incx);
+    if (!alpha_one) v = scale<E, CX>(v, ar, ai);
+    bx[i * NC] = v.r;
+    if constexpr (CX) bx[i * NC + 1] = v.i;
   }
 }
 
 // ---------------------------------------------------------------------------------------
-// gemv, reduction along strided columns: out_c = sum_r op(A[r*lda + c]) * fl(alpha*x_r).
-// One thread per output column (a warp reads 32 consecutive elements of a row); grid =
-// (column blocks of 256, row chunks). With several chunks each thread writes its chunk's
-// partial state to scratch (structure of arrays) and the last CTA to arrive for a column
-// block merges the chunks and finishes the entries.
+// gemv, reduction along strided columns: out_c = sum_r op(A[r*lda + c]) * bx_r.
+// A CTA of 256 threads is G = g.split row groups (1, 2, 4, 8) of T = 256/G threads; thread t
+// of a group owns W adjacent columns (W = 16 bytes / element: s 4, c 2, z 1) and, with g.vec
+// (A 16-byte aligned, lda a multiple of 16 bytes), reads them with one 16-byte load per row,
+// so a warp reads 512 contiguous bytes of a row. grid = (column blocks, row chunks); inside
+// a chunk, group q takes rows q, q+G, ..., K rows per tile. The groups' states are merged
+// through shared memory; with several chunks group 0 writes the chunk's partial states to
+// scratch (structure of arrays) and the last CTA to arrive for a column block merges the
+// chunks (group q takes chunks q, q+G, ...; then the groups merge once more) and finishes.
 // ---------------------------------------------------------------------------------------
+
+// Tree merge of the G row groups' accumulators (renormalised) through shared memory laid out
+// as sm[i * 256 + thread], i < 2F+1; group 0 ends with the merged state. Every thread of the
+// CTA must call it.
+template <typename E, int F>
+__device__ __forceinline__ void merge_groups(Acc<E, F>& a, E* sm, int grp, int t, int G, int T) {
+#pragma unroll 1
+  for (int st = 1; st < G; st <<= 1) {
+    const int m = grp & (2 * st - 1);
+    if (m == st) put_rec<E, F>(a, sm + threadIdx.x, 256);
+    __syncthreads();
+    if (m == 0) merge_rec<E, F, false>(a, sm + (grp + st) * T + t, 256);
+    __syncthreads();
+  }
+}
+
+template <typename E, bool CX>
+struct ColsCfg {
+  static constexpr int NC = CX ? 2 : 1, D = CX ? 2 : 1;
+  static constexpr int W = 16 / ((int)sizeof(E) * NC);   // columns per thread
+  static constexpr int NA = W * NC;                      // accumulators per thread
+  static constexpr int K = 4;                            // rows per tile
+};
+
 template <typename E, bool CX, int F>
-__global__ void __launch_bounds__(256) xgemv_cols_kernel(XGemvArgs<E> g) {
-  constexpr int NC = CX ? 2 : 1, D = CX ? 2 : 1, K = 4;
-  constexpr int REC = NC * (2 * F + 1);
-  const long long c = (long long)blockIdx.x * 256 + threadIdx.x;
+__global__ void __launch_bounds__(256, F <= 3 ? 3 : 2) xgemv_cols_kernel(XGemvArgs<E> g) {
+  using Cfg = ColsCfg<E, CX>;
+  constexpr int NC = Cfg::NC, D = Cfg::D, W = Cfg::W, NA = Cfg::NA, K = Cfg::K;
+  constexpr int PER = 16 / (int)sizeof(E);
+  constexpr int REC = NC * (2 * F + 1);   // scratch record per column
+  __shared__ E sm[(2 * F + 1) * 256];
+  __shared__ unsigned s_last;
+  const int G = g.split, T = 256 / G;
+  const int lgT = __ffs(T) - 1;
+  const int grp = threadIdx.x >> lgT, t = threadIdx.x & (T - 1);
+  const long long cbase = ((long long)blockIdx.x * T + t) * W;
   const int chunk = blockIdx.y, nchunks = gridDim.y;
   const long long rows_per = (g.R + nchunks - 1) / nchunks;
   const long long r0 = (long long)chunk * rows_per < g.R ? (long long)chunk * rows_per : g.R;
   const long long r1 = r0 + rows_per < g.R ? r0 + rows_per : g.R;
-  Acc<E, F> a[NC];
+  const bool full = g.vec && cbase + W <= g.C;   // one 16-byte load covers the W columns
+  Acc<E, F> a[NA];   // column w, component q at w * NC + q
 #pragma unroll
-  for (int q = 0; q < NC; q++) a[q].zero();
-  if (c < g.C) {
+  for (int e = 0; e < NA; e++) a[e].zero();
+  if (cbase < g.C) {
 #pragma unroll 1
-    for (long long b = r0; b < r1; b += K) {
-      E v[NC][K * D];
-      int nv = 0;
+    for (long long b = r0 + grp; b < r1; b += (long long)G * K) {
+      E v[NA][K * D];
+#pragma unroll
+      for (int e = 0; e < NA; e++)
+#pragma unroll
+        for (int d = 0; d < K * D; d++) v[e][d] = E(0);
 #pragma unroll
       for (int k = 0; k < K; k++) {
-        const long long r = b + k;
-#pragma unroll
-        for (int q = 0; q < NC; q++)
-#pragma unroll
-          for (int d = 0; d < D; d++) v[q][k * D + d] = E(0);
+        const long long r = b + (long long)k * G;
         if (r < r1) {
-          Val<E, CX> av = ldv<E, CX>(g.A + r * g.lda * NC, c);
-          if (CX && g.conj) av.i = -av.i;
           Val<E, CX> xv = ldv<E, CX>(g.x, r * g.incx);
           if (!g.alpha_one) xv = scale<E, CX>(xv, g.ar, g.ai);
-          products<E, CX, K * D>(av, xv, v, k);
-          nv = k + 1;
+          const E* rowp = g.A + r * g.lda * NC;
+          E raw[PER];
+          if (full) {
+            ld16<E>(rowp + cbase * NC, raw);
+          } else {
+#pragma unroll
+            for (int w = 0; w < W; w++) {
+              Val<E, CX> av{E(0), E(0)};
+              if (cbase + w < g.C) av = ldv<E, CX>(rowp, cbase + w);
+              raw[w * NC] = av.r;
+              if constexpr (CX) raw[w * NC + NC - 1] = av.i;
+            }
+          }
+#pragma unroll
+          for (int w = 0; w < W; w++) {
+            Val<E, CX> av;
+            av.r = raw[w * NC];
+            av.i = CX ? raw[w * NC + NC - 1] : E(0);
+            if (CX && g.conj) av.i = -av.i;
+            E pv[NC][K * D];
+            products<E, CX, K * D>(av, xv, pv, k);
+#pragma unroll
+            for (int q = 0; q < NC; q++)
+#pragma unroll
+              for (int d = 0; d < D; d++) v[w * NC + q][k * D + d] = pv[q][k * D + d];
+          }
         }
       }
-#pragma unroll
-      for (int q = 0; q < NC; q++) a[q].template tile<K * D>(v[q], nv * D);
+      tileN<E, F, K * D, NA>(a, v);
     }
   }
 #pragma unroll
-  for (int q = 0; q < NC; q++) a[q].renorm();
+  for (int e = 0; e < NA; e++) {
+    a[e].renorm();
+    merge_groups<E, F>(a[e], sm, grp, t, G, T);
+  }
   if (nchunks == 1) {
-    if (c < g.C)
-      finish<E, CX, F>(a, g.mode, g.y + c * g.incy * NC, g.br, g.bi, g.ybin + c * g.incy * 2 * F * NC);
+    if (grp == 0) {
+#pragma unroll
+      for (int w = 0; w < W; w++) {
+        const long long c = cbase + w;
+        if (c < g.C)
+          finish<E, CX, F>(a + w * NC, g.mode, g.y + c * g.incy * NC, g.br, g.bi,
+                           g.ybin + c * g.incy * 2 * F * NC);
+      }
+    }
     return;
   }
-  // partial state of this chunk: element q of the record at scratch[(chunk*REC + q)*C + c]
-  if (c < g.C) {
+  // partial state of this chunk: element q of column c's record at scratch[(chunk*REC + q)*C + c]
+  if (grp == 0) {
 #pragma unroll
-    for (int q = 0; q < NC; q++)
-      put_rec<E, F>(a[q], g.scratch + ((long long)chunk * REC + q * (2 * F + 1)) * g.C + c, g.C);
+    for (int w = 0; w < W; w++) {
+      const long long c = cbase + w;
+      if (c < g.C) {
+#pragma unroll
+        for (int q = 0; q < NC; q++)
+          put_rec<E, F>(a[w * NC + q], g.scratch + ((long long)chunk * REC + q * (2 * F + 1)) * g.C + c,
+                        g.C);
+      }
+    }
   }
-  __shared__ unsigned s_last;
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -306,15 +533,31 @@ __global__ void __launch_bounds__(256) xgemv_cols_kernel(XGemvArgs<E> g) {
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  if (c < g.C) {
 #pragma unroll
-    for (int q = 0; q < NC; q++) {
-      a[q].zero();
+  for (int e = 0; e < NA; e++) a[e].zero();
+#pragma unroll
+  for (int w = 0; w < W; w++) {
+    const long long c = cbase + w;
+    if (c < g.C) {
 #pragma unroll 1
-      for (int ch = 0; ch < nchunks; ch++)
-        merge_rec<E, F, true>(a[q], g.scratch + ((long long)ch * REC + q * (2 * F + 1)) * g.C + c, g.C);
+      for (int ch = grp; ch < nchunks; ch += G) {
+#pragma unroll
+        for (int q = 0; q < NC; q++)
+          merge_rec<E, F, true>(a[w * NC + q],
+                                g.scratch + ((long long)ch * REC + q * (2 * F + 1)) * g.C + c, g.C);
+      }
     }
-    finish<E, CX, F>(a, g.mode, g.y + c * g.incy * NC, g.br, g.bi, g.ybin + c * g.incy * 2 * F * NC);
+  }
+#pragma unroll
+  for (int e = 0; e < NA; e++) merge_groups<E, F>(a[e], sm, grp, t, G, T);
+  if (grp == 0) {
+#pragma unroll
+    for (int w = 0; w < W; w++) {
+      const long long c = cbase + w;
+      if (c < g.C)
+        finish<E, CX, F>(a + w * NC, g.mode, g.y + c * g.incy * NC, g.br, g.bi,
+                         g.ybin + c * g.incy * 2 * F * NC);
+    }
   }
   if (threadIdx.x == 0) g.tickets[blockIdx.x] = 0u;
 }
@@ -437,8 +680,30 @@ __global__ void __launch_bounds__(256) xgemm_kernel(XGemmArgs<E> g) {
 
 template <typename E, bool CX, int F>
 cudaError_t launch_xgemv(const XGemvArgs<E>& g, bool rows, dim3 grid, cudaStream_t s) {
-  if (rows) xgemv_rows_kernel<E, CX, F><<<grid, 256, 0, s>>>(g);
-  else xgemv_cols_kernel<E, CX, F><<<grid, 256, 0, s>>>(g);
+  if (rows) {
+    // persistent over row groups: at most the CTAs that fit on the device at once
+    static int resident = 0;   // CTAs per SM x SMs, per process (one device type)
+    if (resident == 0) {
+      int dev = 0, sms = 0, per = 0;
+      cudaError_t e = cudaGetDevice(&dev);
+      if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, xgemv_rows_kernel<E, CX, F>, 256, 0);
+      if (e != cudaSuccess) return e;
+      resident = (per > 0 ? per : 1) * sms;
+    }
+    if (grid.x > (unsigned)resident) grid.x = (unsigned)resident;
+    xgemv_rows_kernel<E, CX, F><<<grid, 256, 0, s>>>(g);
+  } else {
+    xgemv_cols_kernel<E, CX, F><<<grid, 256, 0, s>>>(g);
+  }
+  return cudaGetLastError();
+}
+
+template <typename E, bool CX>
+cudaError_t launch_xscale(const E* x, long long n, long long incx, E ar, E ai, int alpha_one, E* bx,
+                          int grid, cudaStream_t s) {
+  xscale_kernel<E, CX><<<grid, 256, 0, s>>>(x, n, incx, ar, ai, alpha_one, bx);
   return cudaGetLastError();
 }
 
@@ -462,7 +727,7 @@ cudaError_t launch_xgemm(const XGemmArgs<E>& g, cudaStream_t s) {
 
 template <typename E, bool CX, int F>
 constexpr XOps<E> make_xops() {
-  return XOps<E>{launch_xgemv<E, CX, F>, launch_xgemm<E, CX, F>};
+  return XOps<E>{launch_xgemv<E, CX, F>, launch_xgemm<E, CX, F>, launch_xscale<E, CX>};
 }
 
 }  // namespace xb

@@ -98,6 +98,9 @@ for _t, _b, _sc in (("s", "sbs", c_float), ("z", "zbz", c_vp), ("c", "cbc", c_vp
                                        c_int, c_vp, c_int, _sc, c_vp, c_int])
 _SIGS["sbsconv"] = (None, [c_int, c_float, c_vp])
 _SIGS["zbzconv"] = (None, [c_int, c_vp, c_vp])
+_SIGS["zbzbadd"] = (None, [c_int, c_vp, c_vp])
+_SIGS["cbcbadd"] = (None, [c_int, c_vp, c_vp])
+_SIGS["sbsbaddsq"] = (c_float, [c_int, c_float, c_vp, c_float, c_vp])
 _SIGS["cbcconv"] = (None, [c_int, c_vp, c_vp])
 
 # reference-library names for the shared signatures
@@ -128,6 +131,7 @@ _REF_NAMES = {
     "dindex": "binned_dindex", "sindex": "binned_sindex", "sbsbadd": "binned_sbsbadd",
     "ssbconv": "binned_ssbconv",
     "sbsconv": "binned_sbsconv", "zbzconv": "binned_zbzconv", "cbcconv": "binned_cbcconv",
+    "zbzbadd": "binned_zbzbadd", "cbcbadd": "binned_cbcbadd", "sbsbaddsq": "binned_sbsbaddsq",
 }
 for _t, _b in (("s", "sbs"), ("z", "zbz"), ("c", "cbc")):
     _REF_NAMES[_b + "gemv"] = "binnedBLAS_%sgemv" % _b

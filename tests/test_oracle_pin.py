@@ -536,3 +536,37 @@ def test_port_matches_reference_live_xgemm(port, t):
         n = state_len(t, fold)
         for i in range(nC):
             assert same_state(za[i * n:(i + 1) * n], zb[i * n:(i + 1) * n], fold, comps(t)), (t, order, ta, tb, i)
+
+
+@needs_ref
+def test_port_matches_reference_state_merges(port):
+    """binned_zbzbadd, cbcbadd (the ZBZBADD / CBCBADD operations) and sbsbaddsq (SBSBADDSQ) on
+    states the reference produced, including scales that differ and empty states."""
+    R = ref()
+    rng = np.random.default_rng(808)
+    for trial in range(60):
+        fold = int(rng.integers(2, 9))
+        dist = ["uniform", "normal", "loguniform", "illcond", "huge", "tiny"][trial % 6]
+        na, nb = int(rng.integers(0, 3000)), int(rng.integers(0, 3000))
+        for kind in "zc":
+            cd = np.complex128 if kind == "z" else np.complex64
+            xa, xb = gen_complex(dist, na + 1, trial, cd), gen_complex(dist, nb + 1, trial + 1, cd)
+            za, zb = binned_zeros(fold, kind), binned_zeros(fold, kind)
+            if kind == "z":
+                R.zbzsum(fold, na, ptr(xa), 1, ptr(za))
+                R.zbzsum(fold, nb, ptr(xb), 1, ptr(zb))
+            else:
+                R.cbcsum(fold, na, ptr(xa), 1, ptr(za))
+                R.cbcsum(fold, nb, ptr(xb), 1, ptr(zb))
+            p, q = zb.copy(), zb.copy()
+            getattr(port, kind + "b" + kind + "badd")(fold, ptr(za), ptr(p))
+            getattr(R, kind + "b" + kind + "badd")(fold, ptr(za), ptr(q))
+            assert same_state(p, q, fold, 2), (kind, trial)
+        xa, xb = gen(dist, na + 1, trial, np.float32), gen(dist, nb + 1, trial + 2, np.float32)
+        za, zb = binned_zeros(fold, "s"), binned_zeros(fold, "s")
+        sa = R.sbsssq(fold, na, ptr(xa), 1, 0.0, ptr(za))
+        sb = R.sbsssq(fold, nb, ptr(xb), 1, 0.0, ptr(zb))
+        p, q = zb.copy(), zb.copy()
+        s1 = port.sbsbaddsq(fold, sa, ptr(za), sb, ptr(p))
+        s2 = R.sbsbaddsq(fold, sa, ptr(za), sb, ptr(q))
+        assert same_value(np.float32(s1), np.float32(s2)) and same_state(p, q, fold), trial
