@@ -280,8 +280,36 @@ __global__ void __launch_bounds__(256, F <= 3 ? 3 : 2) xgemv_rows_kernel(XGemvAr
     long long ce = c0;   // start of the element path
     if (g.vec) {
       const long long nvec = (c1 - c0) / VE;
+      const long long nfull = nvec / (32 * NV) * (32 * NV);   // vectors in whole warp tiles
+      const E* ap = row + c0 * NC;
+      const E* xp = g.x + c0 * NC;
+      // whole warp tiles: every lane's NV vectors exist; all loads issued before the math
 #pragma unroll 1
-      for (long long vb = lane; vb < nvec; vb += 32 * NV) {
+      for (long long vb = lane; vb < nfull; vb += 32 * NV) {
+        E av[NV][PER], xv[NV][PER];
+#pragma unroll
+        for (int j = 0; j < NV; j++) {
+          ld16<E>(ap + (vb + 32 * j) * PER, av[j]);
+          ld16<E>(xp + (vb + 32 * j) * PER, xv[j]);
+        }
+        E v[NC][KD];
+#pragma unroll
+        for (int j = 0; j < NV; j++)
+#pragma unroll
+          for (int e = 0; e < VE; e++) {
+            Val<E, CX> aa, xx;
+            aa.r = av[j][e * NC];
+            xx.r = xv[j][e * NC];
+            aa.i = CX ? av[j][e * NC + NC - 1] : E(0);
+            xx.i = CX ? xv[j][e * NC + NC - 1] : E(0);
+            if (CX && g.conj) aa.i = -aa.i;
+            products<E, CX, KD>(aa, xx, v, j * VE + e);
+          }
+        deposit_tile<E, CX, F, KD>(a, v, KD);
+      }
+      // the last, partial warp tile
+#pragma unroll 1
+      for (long long vb = nfull + lane; vb < nvec; vb += 32 * NV) {
         E v[NC][KD];
 #pragma unroll
         for (int q = 0; q < NC; q++)
@@ -449,50 +477,59 @@ __global__ void __launch_bounds__(256, F <= 3 ? 3 : 2) xgemv_cols_kernel(XGemvAr
   Acc<E, F> a[NA];   // column w, component q at w * NC + q
 #pragma unroll
   for (int e = 0; e < NA; e++) a[e].zero();
-  if (cbase < g.C) {
-#pragma unroll 1
-    for (long long b = r0 + grp; b < r1; b += (long long)G * K) {
-      E v[NA][K * D];
+  // one tile of K rows b, b+G, ...; GUARD: rows past r1 may occur (zeros deposit nothing)
+  auto tile = [&](long long b, bool guard) {
+    E raw[K][PER];
+    Val<E, CX> xv[K];
 #pragma unroll
-      for (int e = 0; e < NA; e++)
+    for (int k = 0; k < K; k++) {
+      const long long r = b + (long long)k * G;
+      xv[k].r = E(0);
+      xv[k].i = E(0);
 #pragma unroll
-        for (int d = 0; d < K * D; d++) v[e][d] = E(0);
-#pragma unroll
-      for (int k = 0; k < K; k++) {
-        const long long r = b + (long long)k * G;
-        if (r < r1) {
-          Val<E, CX> xv = ldv<E, CX>(g.x, r * g.incx);
-          if (!g.alpha_one) xv = scale<E, CX>(xv, g.ar, g.ai);
-          const E* rowp = g.A + r * g.lda * NC;
-          E raw[PER];
-          if (full) {
-            ld16<E>(rowp + cbase * NC, raw);
-          } else {
-#pragma unroll
-            for (int w = 0; w < W; w++) {
-              Val<E, CX> av{E(0), E(0)};
-              if (cbase + w < g.C) av = ldv<E, CX>(rowp, cbase + w);
-              raw[w * NC] = av.r;
-              if constexpr (CX) raw[w * NC + NC - 1] = av.i;
-            }
-          }
+      for (int i = 0; i < PER; i++) raw[k][i] = E(0);
+      if (!guard || r < r1) {
+        xv[k] = ldv<E, CX>(g.x, r * g.incx);
+        const E* rowp = g.A + r * g.lda * NC;
+        if (full) {
+          ld16<E>(rowp + cbase * NC, raw[k]);
+        } else {
 #pragma unroll
           for (int w = 0; w < W; w++) {
-            Val<E, CX> av;
-            av.r = raw[w * NC];
-            av.i = CX ? raw[w * NC + NC - 1] : E(0);
-            if (CX && g.conj) av.i = -av.i;
-            E pv[NC][K * D];
-            products<E, CX, K * D>(av, xv, pv, k);
-#pragma unroll
-            for (int q = 0; q < NC; q++)
-#pragma unroll
-              for (int d = 0; d < D; d++) v[w * NC + q][k * D + d] = pv[q][k * D + d];
+            Val<E, CX> av{E(0), E(0)};
+            if (cbase + w < g.C) av = ldv<E, CX>(rowp, cbase + w);
+            raw[k][w * NC] = av.r;
+            if constexpr (CX) raw[k][w * NC + NC - 1] = av.i;
           }
         }
       }
-      tileN<E, F, K * D, NA>(a, v);
     }
+    E v[NA][K * D];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      if (!g.alpha_one) xv[k] = scale<E, CX>(xv[k], g.ar, g.ai);
+#pragma unroll
+      for (int w = 0; w < W; w++) {
+        Val<E, CX> av;
+        av.r = raw[k][w * NC];
+        av.i = CX ? raw[k][w * NC + NC - 1] : E(0);
+        if (CX && g.conj) av.i = -av.i;
+        E pv[NC][K * D];
+        products<E, CX, K * D>(av, xv[k], pv, k);
+#pragma unroll
+        for (int q = 0; q < NC; q++)
+#pragma unroll
+          for (int d = 0; d < D; d++) v[w * NC + q][k * D + d] = pv[q][k * D + d];
+      }
+    }
+    tileN<E, F, K * D, NA>(a, v);
+  };
+  if (cbase < g.C) {
+    long long b = r0 + grp;
+    // whole tiles: all K rows exist; loads issued before the math
+#pragma unroll 1
+    for (; b + (long long)(K - 1) * G < r1; b += (long long)G * K) tile(b, false);
+    if (b < r1) tile(b, true);
   }
 #pragma unroll
   for (int e = 0; e < NA; e++) {
