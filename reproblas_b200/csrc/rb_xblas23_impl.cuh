@@ -17,6 +17,8 @@
 // each product and the sum rounded separately; beta*y is formed the same way
 // (rzgemv.c:56-58).
 #pragma once
+#include <atomic>
+
 #include "rb_binned.cuh"
 #include "rb_kernels.cuh"
 
@@ -718,16 +720,21 @@ __global__ void __launch_bounds__(256) xgemm_kernel(XGemmArgs<E> g) {
 template <typename E, bool CX, int F>
 cudaError_t launch_xgemv(const XGemvArgs<E>& g, bool rows, dim3 grid, cudaStream_t s) {
   if (rows) {
-    // persistent over row groups: at most the CTAs that fit on the device at once
-    static int resident = 0;   // CTAs per SM x SMs, per process (one device type)
+    // all warps resident at once: at most the CTAs that fit on the device (per device)
+    constexpr int kMaxDevices = 64;
+    static std::atomic<int> cache[kMaxDevices];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    int resident = dev < kMaxDevices ? cache[dev].load(std::memory_order_relaxed) : 0;
     if (resident == 0) {
-      int dev = 0, sms = 0, per = 0;
-      cudaError_t e = cudaGetDevice(&dev);
-      if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      int sms = 0, per = 0;
+      e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
       if (e == cudaSuccess)
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, xgemv_rows_kernel<E, CX, F>, 256, 0);
       if (e != cudaSuccess) return e;
       resident = (per > 0 ? per : 1) * sms;
+      if (dev < kMaxDevices) cache[dev].store(resident, std::memory_order_relaxed);
     }
     if (grid.x > (unsigned)resident) grid.x = (unsigned)resident;
     xgemv_rows_kernel<E, CX, F><<<grid, 256, 0, s>>>(g);
