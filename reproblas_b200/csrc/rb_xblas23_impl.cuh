@@ -218,28 +218,28 @@ struct RowsCfg {
 // Even split of `total` row-major elements of rows of C over nw warps: warp w starts at
 // floor(w*total/nw), rounded down to a multiple of VE within its row.
 struct RowSplit {
-  long long total, C, q, rem;
-  int nw, ve;
+  long long total, C, q;
+  unsigned rem, nw;
+  int ve;
   __device__ __forceinline__ RowSplit(long long total_, long long C_, int nw_, int ve_)
-      : total(total_), C(C_), nw(nw_), ve(ve_) {
-    q = total / nw;
-    rem = total - q * nw;
+      : total(total_), C(C_), nw((unsigned)nw_), ve(ve_) {
+    q = total / nw_;
+    rem = (unsigned)(total - q * nw_);
+  }
+  // e / C for 0 <= e < 2^53: a double estimate corrected to the exact quotient
+  __device__ __forceinline__ long long row_of(long long e) const {
+    long long r = (long long)((double)e / (double)C);
+    while (r > 0 && r * C > e) r--;
+    while ((r + 1) * C <= e) r++;
+    return r;
   }
   __device__ __forceinline__ long long start(long long w) const {
-    if (w >= nw) return total;
-    const long long b = w * q + (w * rem) / nw;   // floor(w * total / nw) without overflow
-    const long long r = b / C;
+    if (w >= (long long)nw) return total;
+    // floor(w * total / nw) = w*q + floor(w*rem / nw), with w*rem < nw^2 < 2^32
+    const long long b = w * q + (long long)(((unsigned)w * rem) / nw);
+    const long long r = row_of(b);
     const long long c = b - r * C;
     return r * C + (c - c % ve);
-  }
-  // the warp whose range holds element e (0 <= e < total)
-  __device__ __forceinline__ long long owner(long long e) const {
-    long long w = (long long)((double)e * (double)nw / (double)total);
-    if (w >= nw) w = nw - 1;
-    if (w < 0) w = 0;
-    for (int i = 0; i < 64 && w + 1 < nw && start(w + 1) <= e; i++) w++;
-    for (int i = 0; i < 64 && w > 0 && start(w) > e; i++) w--;
-    return w;
   }
 };
 
@@ -272,7 +272,7 @@ __global__ void __launch_bounds__(256, F <= 3 ? 3 : 2) xgemv_rows_kernel(XGemvAr
   const long long b0 = sp.start(gwarp), b1 = sp.start(gwarp + 1);
 #pragma unroll 1
   for (long long pos = b0; pos < b1;) {
-    const long long r = pos / g.C;
+    const long long r = sp.row_of(pos);
     const long long c0 = pos - r * g.C;
     const long long c1 = (r + 1) * g.C <= b1 ? g.C : b1 - r * g.C;
     Acc<E, F> a[NC];
@@ -372,25 +372,31 @@ __global__ void __launch_bounds__(256, F <= 3 ? 3 : 2) xgemv_rows_kernel(XGemvAr
     }
     bool done = c0 == 0 && c1 == g.C;   // the whole row is this warp's
     if (!done) {
+      // part of a cut row: record in slot 2w (the warp's first row) or 2w+1 (its last row);
+      // the row's ticket counts finished elements, so the warp that brings it to C completes it
       const long long slot = pos == b0 ? 2 * gwarp : 2 * gwarp + 1;
-      unsigned tk = 0;
+      unsigned old = 0;
       if (lane == 0) {
         E* rec = g.scratch + slot * REC;
 #pragma unroll
         for (int q = 0; q < NC; q++) put_rec<E, F>(a[q], rec + q * (2 * F + 1), 1);
         __threadfence();
-        tk = atomicAdd(g.tickets + r, 1u);
+        old = atomicAdd(g.tickets + r, (unsigned)(c1 - c0));
       }
-      tk = __shfl_sync(0xffffffffu, tk, 0);
-      const long long fw = sp.owner(r * g.C), lw = sp.owner(r * g.C + g.C - 1);
-      if ((long long)tk == lw - fw) {
+      old = __shfl_sync(0xffffffffu, old, 0);
+      if ((long long)old + (c1 - c0) == g.C) {
         __threadfence();
+        // the row's parts belong to the contiguous warps around this one whose ranges meet it
+        const long long rs = r * g.C, re = rs + g.C;
+        long long fw = gwarp, lw = gwarp;
+        while (fw > 0 && sp.start(fw) > rs) fw--;
+        while (lw + 1 < nwe && sp.start(lw + 1) < re) lw++;
         // lanes take the parts of warps fw + lane, fw + lane + 32, ...; then a butterfly
 #pragma unroll
         for (int q = 0; q < NC; q++) a[q].zero();
 #pragma unroll 1
         for (long long v = fw + lane; v <= lw; v += 32) {
-          const long long vs = sp.start(v) / g.C == r ? 2 * v : 2 * v + 1;
+          const long long vs = sp.start(v) >= rs ? 2 * v : 2 * v + 1;
 #pragma unroll
           for (int q = 0; q < NC; q++)
             merge_rec<E, F, true>(a[q], g.scratch + vs * REC + q * (2 * F + 1), 1);
