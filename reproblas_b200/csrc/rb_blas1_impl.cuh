@@ -125,8 +125,10 @@ template <typename T, int F, int OP>
 struct Red1 {
   Acc<T, F> a;
   double scl;   // sum of squares: current power-of-two scale (0 = none yet)
+  T inv;        // sum of squares: 1/scl, valid while inv_of == scl
+  double inv_of;
 
-  __device__ __forceinline__ void init() { a.zero(); scl = 0.0; }
+  __device__ __forceinline__ void init() { a.zero(); scl = 0.0; inv_of = -1.0; }
 
   // Deposit K elements (x[k], y[k]) of which the first nv are real.
   template <int K>
@@ -173,7 +175,12 @@ struct Red1 {
       scl = (double)nscl;
     }
     // x * (1/scale), squared (depositSSq.py:17-26); 1/scale is an exact power of two
-    const T inv = bdiv(T(1), (T)scl);
+    // FP32: 1/scl kept between tiles (the division dominated the FP32 tile); FP64 recomputes
+    // it, which keeps the FP64 kernel's registers within its 4-CTA budget
+    if (sizeof(T) == 8 || inv_of != scl) {
+      inv = bdiv(T(1), (T)scl);
+      inv_of = scl;
+    }
     T v[K];
 #pragma unroll
     for (int k = 0; k < K; k++) {
@@ -195,6 +202,7 @@ struct Red1 {
     Red1 o;
     o.a = a.shfl_xor(mask);
     o.scl = __shfl_xor_sync(0xffffffffu, scl, mask);
+    o.inv_of = -1.0;
     return o;
   }
 
@@ -211,6 +219,7 @@ struct Red1 {
     for (int i = 0; i < F; i++) { a.pri[i] = ldrec<G>(r + i); a.car[i] = ldrec<G>(r + F + i); }
     a.flags = (unsigned)BT<T>::bits(ldrec<G>(r + 2 * F));
     scl = (double)ldrec<G>(r + 2 * F + 1);
+    inv_of = -1.0;
     a.set_idx_from_pri();
     a.deposits = 0;
   }
