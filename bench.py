@@ -62,6 +62,9 @@ def parse():
     p.add_argument("--profile-m", type=int, default=0,
                    help="rows of A for the gemv profile cases (default: --profile-n)")
     p.add_argument("--profile-slices", type=int, default=7)
+    p.add_argument("--sweep", action="store_true",
+                   help="only run the BLAS1 sweep (N = 2^10..2^28 in powers of 4, folds 2/3/4, "
+                        "four value distributions) and print its JSON table")
     return p.parse_args()
 
 
@@ -425,6 +428,69 @@ def blas1_sweep(torch, rb):
     return out
 
 
+def sweep_values(torch, dist, n, g):
+    """Device vector of n FP64 values: uniform(-1,1), standard normal, log-uniform magnitude
+    2^U(-300,300) with random sign, or ill-conditioned (x, -x) pairs plus n/16 entries of
+    magnitude 1e-12, shuffled."""
+    if dist == "uniform":
+        return torch.rand(n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    if dist == "normal":
+        return torch.randn(n, dtype=torch.float64, device="cuda", generator=g)
+    if dist == "loguniform":
+        e = torch.rand(n, dtype=torch.float64, device="cuda", generator=g) * 600 - 300
+        sgn = torch.randint(0, 2, (n,), device="cuda", generator=g).double() * 2 - 1
+        return torch.exp2(e) * sgn
+    half = n // 2
+    a = torch.rand(half, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    x = torch.cat([a, -a, torch.zeros(n - 2 * half, dtype=torch.float64, device="cuda")])
+    k = n // 16
+    idx = torch.randperm(n, device="cuda", generator=g)[:k]
+    x[idx] = 1e-12
+    return x[torch.randperm(n, device="cuda", generator=g)]
+
+
+def blas1_full_sweep():
+    """The BLAS1 sweep: dsum, ddot, dnrm2 (FP64), ssum, sdot (FP32), zsum, zdotc (complex128)
+    at N = 2^10, 2^12, ..., 2^28 elements (complex: N/2 complex elements over the same bytes),
+    folds 2, 3, 4, distributions uniform / normal / log-uniform / ill-conditioned; inputs
+    resident in HBM; CUDA-event time per call over back-to-back calls (each call also reads its
+    8-byte result back, as reproBLAS_r* do). Prints one JSON object: per routine, distribution
+    and fold, {log2 N: [GB/s, us per call]}."""
+    import torch
+    import reproblas_b200 as rb
+    g = torch.Generator(device="cuda").manual_seed(11)
+    sizes = list(range(10, 29, 2))
+    table = {}
+    nmax = 1 << 28
+    for dist in ("uniform", "normal", "loguniform", "illcond"):
+        x = sweep_values(torch, dist, nmax, g)
+        y = sweep_values(torch, dist, nmax, g)
+        xf = x.float()
+        yf = y.float()
+        for fold in (2, 3, 4):
+            cases = {
+                "dsum": (8, lambda n: rb.call("reproBLAS_rdsum", fold, n, x, 1)),
+                "ddot": (16, lambda n: rb.call("reproBLAS_rddot", fold, n, x, 1, y, 1)),
+                "dnrm2": (8, lambda n: rb.call("reproBLAS_rdnrm2", fold, n, x, 1)),
+                "ssum": (4, lambda n: rb.call("reproBLAS_rssum", fold, n, xf, 1)),
+                "sdot": (8, lambda n: rb.call("reproBLAS_rsdot", fold, n, xf, 1, yf, 1)),
+                "zsum": (8, lambda n: rb.call("reproBLAS_rzsum_sub", fold, n // 2, x, 1, out)),
+                "zdotc": (16, lambda n: rb.call("reproBLAS_rzdotc_sub", fold, n // 2, x, 1, y, 1, out)),
+            }
+            out = torch.zeros(2, dtype=torch.float64, device="cuda")
+            for name, (bpe, fn) in cases.items():
+                row = {}
+                for lg in sizes:
+                    n = 1 << lg
+                    reps = 20 if lg >= 24 else 200
+                    t = _event_time(torch, lambda: fn(n), reps, warm=3)
+                    row[lg] = [round(bpe * n / t / 1e9, 1), round(t * 1e6, 2)]
+                table.setdefault(name, {}).setdefault(dist, {})[fold] = row
+        del x, y, xf, yf
+    print(json.dumps({"blas1_sweep": table, "unit": "[GB/s, us per call]",
+                      "peak_gbs": peaks()[0], "peak_source": peaks()[1]}))
+
+
 def batched_case(torch, rb, rng, profile_steps=0, total_log2=28):
     """Batched ragged configuration: 10,000 ddot segments with log-uniform lengths (drawn as
     floor(2^U(0,20)), then scaled so the total is ~2^28 elements, normal values) and 512
@@ -723,6 +789,9 @@ def main():
     args = parse()
     if args.profile_kernel:
         profile_case(args)
+        return
+    if args.sweep:
+        blas1_full_sweep()
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
