@@ -110,11 +110,17 @@ bool run_blas1(const Blas1Req& r) {
   if (!w) return false;
   cudaStream_t s = w->stream;
 
+  const bool x_dev = n == 0 || on_device(r.x);
+  const bool y_dev = !dot || n == 0 || on_device(r.y);
+  // one launch over device operands without a caller state: the kernel starts from the empty
+  // state itself, and a value result is stored straight into the pinned result slot
+  const bool direct = x_dev && y_dev && !r.acc;
+
   // --- accumulator placement ---
   const size_t acc_bytes = (size_t)comps(r.type) * 2 * r.fold * rb_;
   const bool acc_dev = r.acc && on_device(r.acc);
-  void* dacc = acc_dev ? r.acc : (void*)w->dacc();
-  if (!acc_dev) {
+  void* dacc = direct ? nullptr : acc_dev ? r.acc : (void*)w->dacc();
+  if (!acc_dev && !direct) {
     if (r.acc) {
       std::memcpy(w->hacc(), r.acc, acc_bytes);
       if (!cuda_ok(cudaMemcpyAsync(dacc, w->hacc(), acc_bytes, cudaMemcpyHostToDevice, s), "copy accumulator")) return false;
@@ -122,13 +128,16 @@ bool run_blas1(const Blas1Req& r) {
       return false;
     }
   }
-  const bool ssq = comps(r.type) == 1 && r.op == kOpSsq;
+  // the scale travels with a caller's state (in) or to the caller (out); the value path of
+  // a direct launch needs neither
+  const bool ssq = comps(r.type) == 1 && r.op == kOpSsq && !(direct && !r.scale_out);
   if (ssq) {
     *w->hscale() = r.scale_in;
     if (!cuda_ok(cudaMemcpyAsync(w->dscale(), w->hscale(), 8, cudaMemcpyHostToDevice, s), "copy scale")) return false;
   }
   const bool res_dev = r.result && on_device(r.result);
-  void* dres = r.result ? (res_dev ? r.result : w->dresult()) : nullptr;
+  const bool res_mapped = r.result && !res_dev && direct;   // kernel writes hresult() itself
+  void* dres = r.result ? (res_dev ? r.result : res_mapped ? w->hresult_dev() : w->dresult()) : nullptr;
 
   Blas1Args a{};
   a.scratch = w->scratch;
@@ -138,9 +147,6 @@ bool run_blas1(const Blas1Req& r) {
 
   LaunchShape ls = launch_shape();
   const int threads = ls.threads > 0 ? ls.threads : 256;
-
-  const bool x_dev = n == 0 || on_device(r.x);
-  const bool y_dev = !dot || n == 0 || on_device(r.y);
 
   if (x_dev && y_dev) {
     // one launch over the device-resident vectors
@@ -223,8 +229,9 @@ bool run_blas1(const Blas1Req& r) {
     need_sync = true;
   }
   if (r.result && !res_dev) {
-    if (!cuda_ok(cudaMemcpyAsync(w->hresult(), dres, comps(r.type) * rb_ + (r.type == 's' ? 0 : 0),
-                                 cudaMemcpyDeviceToHost, s), "copy result"))
+    if (!res_mapped &&
+        !cuda_ok(cudaMemcpyAsync(w->hresult(), dres, comps(r.type) * rb_, cudaMemcpyDeviceToHost, s),
+                 "copy result"))
       return false;
     need_sync = true;
   }

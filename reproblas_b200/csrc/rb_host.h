@@ -51,6 +51,7 @@ struct Workspace {
   size_t records_bytes = 0;
   unsigned char* dsmall = nullptr;      // device: accumulator / scale / result slots
   unsigned char* hsmall = nullptr;      // pinned host mirror of dsmall
+  unsigned char* hsmall_dev = nullptr;  // the device's address of hsmall (mapped pinned memory)
   static constexpr size_t kSmallBytes = 4096;
   // staging ring: kRing slots, each with up to two operand buffers of chunk_bytes
   static constexpr int kRing = 3;
@@ -75,6 +76,7 @@ struct Workspace {
   double* hacc() { return (double*)hsmall; }
   double* hscale() { return (double*)(hsmall + 1024); }
   void* hresult() { return (void*)(hsmall + 1088); }
+  void* hresult_dev() { return (void*)(hsmall_dev + 1088); }   // hresult() as kernels address it
 
   bool ensure_ring(size_t chunk);
   bool ensure_big(size_t bytes);

@@ -148,6 +148,9 @@ static bool init_workspace(Workspace* w, int dev, cudaStream_t s, int sms) {
       !cuda_ok(cudaMemset(w->dsmall, 0, Workspace::kSmallBytes), "cudaMemset"))
     return false;
   if (!cuda_ok(cudaMallocHost(&w->hsmall, Workspace::kSmallBytes), "cudaMallocHost")) return false;
+  // the device's address of the pinned slots (kernels store value results straight there)
+  if (!cuda_ok(cudaHostGetDevicePointer((void**)&w->hsmall_dev, w->hsmall, 0), "cudaHostGetDevicePointer"))
+    return false;
   if (!cuda_ok(cudaStreamCreateWithFlags(&w->copy_stream, cudaStreamNonBlocking),
                "cudaStreamCreate"))
     return false;
