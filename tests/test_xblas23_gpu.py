@@ -234,3 +234,26 @@ def test_xblas23_errors(cuda, rb):
     one = np.array([1.0, 0.0], np.float32)
     with pytest.raises(rb.ReproBLASError):
         rb.call("reproBLAS_rcgemm", 3, "r", "n", "n", 2, 2, 2, one, A, 0, A, 2, one, y, 2)
+
+
+@pytest.mark.parametrize("t", ["s", "z", "c"])
+def test_xgemv_extreme_shapes(cuda, rb, port, t):
+    """Shapes at the ends of the row split: one row of 200000 elements (every warp of the split
+    holds a part of it; the completing warp merges ~190 parts), 3 rows of 100000, and 300000
+    rows of 3 elements (many rows per warp); both reductions, value form."""
+    for M, N in [(1, 200000), (3, 100000), (300000, 3)]:
+        for ta in "nc":
+            A = _ops(t, M * N, M + N, "normal")
+            lenx, leny = (N, M) if ta == "n" else (M, N)
+            X = _ops(t, lenx, 7, "loguniform")
+            Y = _ops(t, leny, 8, "normal")
+            al = 1.5 if t == "s" else 1.5 - 0.25j
+            want = Y.copy()
+            lib_gemv(port, t, 3, "r", ta, M, N, al, A, N, X, 1, 0.5, want, 1)
+            gd = dview(cuda, t, Y)
+            rb_gemv(rb, t, 3, "r", ta, M, N, al, dview(cuda, t, A), N, dview(cuda, t, X), 1, 0.5, gd, 1)
+            assert same_value(real_view(t, host_of(t, gd, Y)), real_view(t, want)), (t, M, N, ta)
+            # twice in a row: the row tickets are back at zero after a call
+            gd2 = dview(cuda, t, Y)
+            rb_gemv(rb, t, 3, "r", ta, M, N, al, dview(cuda, t, A), N, dview(cuda, t, X), 1, 0.5, gd2, 1)
+            assert same_value(real_view(t, host_of(t, gd2, Y)), real_view(t, want)), (t, M, N, ta, 2)
