@@ -337,7 +337,15 @@ template <typename T, int F> struct Acc {
       return;
     }
     int shift = idx - X.idx;
-    if (shift > 0) {
+    if (shift == 0) {
+      // same bins (the common case of merges between neighbouring threads): the arithmetic
+      // of the aligned branch below without its shift selection
+#pragma unroll
+      for (int i = 0; i < F; i++) {
+        pri[i] = B::add(pri[i], B::sub(X.pri[i], B::bin(X.idx + i)));
+        car[i] = B::add(car[i], X.car[i]);
+      }
+    } else if (shift > 0) {
       // Y moves to X's (coarser) index
 #pragma unroll
       for (int i = F - 1; i >= 0; i--) {
