@@ -462,7 +462,7 @@ struct ColsCfg {
   static constexpr int NC = CX ? 2 : 1, D = CX ? 2 : 1;
   static constexpr int W = 16 / ((int)sizeof(E) * NC);   // columns per thread
   static constexpr int NA = W * NC;                      // accumulators per thread
-  static constexpr int K = 4;                            // rows per tile
+  static constexpr int K = (CX && sizeof(E) == 4) ? 2 : 4;   // rows per tile (c: 2 keeps it unspilled)
 };
 
 template <typename E, bool CX, int F>
