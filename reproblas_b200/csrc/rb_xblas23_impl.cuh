@@ -210,7 +210,7 @@ struct RowsCfg {
   static constexpr int NC = CX ? 2 : 1, D = CX ? 2 : 1;
   static constexpr int PER = 16 / (int)sizeof(E);   // reals per 16-byte vector
   static constexpr int VE = PER / NC;               // elements per vector: z 1, c 2, s 4
-  static constexpr int NV = CX ? 2 : 4;             // vectors per lane per tile
+  static constexpr int NV = (CX && sizeof(E) == 4) ? 2 : 4;   // vectors per lane per tile
   static constexpr int KE = NV * VE;                // elements per lane per tile
   static constexpr int KD = KE * D;                 // deposits per component per tile
 };
@@ -244,7 +244,8 @@ struct RowSplit {
 };
 
 template <typename E, bool CX, int F>
-__global__ void __launch_bounds__(256, F <= 3 ? 3 : 2) xgemv_rows_kernel(XGemvArgs<E> g) {
+__global__ void __launch_bounds__(256, (F <= 3 && !(CX && sizeof(E) == 8)) ? 3 : 2)
+    xgemv_rows_kernel(XGemvArgs<E> g) {
   using Cfg = RowsCfg<E, CX>;
   constexpr int NC = Cfg::NC, D = Cfg::D, PER = Cfg::PER, VE = Cfg::VE, NV = Cfg::NV;
   constexpr int KD = Cfg::KD, K = 4;
