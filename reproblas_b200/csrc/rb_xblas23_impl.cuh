@@ -463,13 +463,19 @@ struct ColsCfg {
   static constexpr int NC = CX ? 2 : 1, D = CX ? 2 : 1;
   static constexpr int W = 16 / ((int)sizeof(E) * NC);   // columns per thread
   static constexpr int NA = W * NC;                      // accumulators per thread
-  static constexpr int K = (CX && sizeof(E) == 4) ? 2 : 4;   // rows per tile (c: 2 keeps it unspilled)
+  static constexpr bool C32 = CX && sizeof(E) == 4, Z = CX && sizeof(E) == 8;
+  // rows per tile: c 2 (keeps it unspilled), z 8 up to fold 3 (at 2 CTAs per SM), else 4
+  template <int F> __host__ __device__ static constexpr int rows_per_tile() {
+    return C32 ? 2 : (Z && F <= 3) ? 8 : 4;
+  }
+  static constexpr int MIN_CTAS = Z ? 2 : 3;              // resident CTAs per SM the kernel is built for
 };
 
 template <typename E, bool CX, int F>
-__global__ void __launch_bounds__(256, F <= 3 ? 3 : 2) xgemv_cols_kernel(XGemvArgs<E> g) {
+__global__ void __launch_bounds__(256, F <= 3 ? ColsCfg<E, CX>::MIN_CTAS : 2) xgemv_cols_kernel(XGemvArgs<E> g) {
   using Cfg = ColsCfg<E, CX>;
-  constexpr int NC = Cfg::NC, D = Cfg::D, W = Cfg::W, NA = Cfg::NA, K = Cfg::K;
+  constexpr int NC = Cfg::NC, D = Cfg::D, W = Cfg::W, NA = Cfg::NA;
+  constexpr int K = Cfg::template rows_per_tile<F>();
   constexpr int PER = 16 / (int)sizeof(E);
   constexpr int REC = NC * (2 * F + 1);   // scratch record per column
   __shared__ E sm[(2 * F + 1) * 256];
