@@ -121,8 +121,8 @@ bool run_xgemv(const XGemvReq<E, CX>& q) {
     if (!w->ensure_tickets((size_t)nout)) return false;
   } else {
     const long long W = (long long)(16 / es);
-    // resident CTAs: the column kernel is built for 3 per SM up to fold 3 (2 for double complex)
-    const long long slots = (long long)di.sms * (q.fold <= 3 && !(CX && sizeof(E) == 8) ? 3 : 2);
+    // resident CTAs: the column kernel is built for 3 per SM up to fold 3 (2 for complex)
+    const long long slots = (long long)di.sms * (q.fold <= 3 && !CX ? 3 : 2);
     long long best = -1;
     for (int G = 1; G <= 8; G *= 2) {
       const long long cols = (256 / G) * W;

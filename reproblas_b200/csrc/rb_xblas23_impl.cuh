@@ -464,11 +464,11 @@ struct ColsCfg {
   static constexpr int W = 16 / ((int)sizeof(E) * NC);   // columns per thread
   static constexpr int NA = W * NC;                      // accumulators per thread
   static constexpr bool C32 = CX && sizeof(E) == 4, Z = CX && sizeof(E) == 8;
-  // rows per tile: c 2 (keeps it unspilled), z 8 up to fold 3 (at 2 CTAs per SM), else 4
+  // rows per tile: z 8 up to fold 3, c and s 4 (complex at 2 CTAs per SM, real at 3)
   template <int F> __host__ __device__ static constexpr int rows_per_tile() {
-    return C32 ? 2 : (Z && F <= 3) ? 8 : 4;
+    return (Z && F <= 3) ? 8 : 4;
   }
-  static constexpr int MIN_CTAS = Z ? 2 : 3;              // resident CTAs per SM the kernel is built for
+  static constexpr int MIN_CTAS = CX ? 2 : 3;             // resident CTAs per SM the kernel is built for
 };
 
 template <typename E, bool CX, int F>
