@@ -299,6 +299,60 @@ void binnedBLAS_cbcdotc(const int fold, const int N, const void *X, const int in
 void binnedBLAS_cbcdotu(const int fold, const int N, const void *X, const int incX,
                         const void *Y, const int incY, float_complex_binned *Z);
 
+/* The manual-layout forms, include/binnedBLAS.h:48-85 (src/binnedBLAS/dmdsum.ccog,
+ * dmdasum.ccog, dmdssq.ccog, dmddot.ccog, zmzsum.ccog, dmzasum.ccog, dmzssq.ccog,
+ * zmzdotu.ccog, zmzdotc.ccog, smssum.ccog, smsasum.ccog, smsssq.ccog, smsdot.ccog,
+ * cmcsum.ccog, smcasum.ccog, smcssq.ccog, cmcdotu.ccog, cmcdotc.ccog): the reductions of the
+ * ?b? forms above on a state held as a primary array and a carry array with their own
+ * (positive) strides; for complex states component c of element i is at [2*i*inc + c].
+ * Same bits as the ?b? form on the gathered state; host or device state arrays. */
+void binnedBLAS_dmdsum(const int fold, const int N, const double *X, const int incX,
+                       double *priY, const int incpriY, double *carY, const int inccarY);
+void binnedBLAS_dmdasum(const int fold, const int N, const double *X, const int incX,
+                        double *priY, const int incpriY, double *carY, const int inccarY);
+double binnedBLAS_dmdssq(const int fold, const int N, const double *X, const int incX,
+                         const double scaleY, double *priY, const int incpriY, double *carY,
+                         const int inccarY);
+void binnedBLAS_dmddot(const int fold, const int N, const double *X, const int incX,
+                       const double *Y, const int incY, double *manZ, const int incmanZ,
+                       double *carZ, const int inccarZ);
+void binnedBLAS_zmzsum(const int fold, const int N, const void *X, const int incX, double *priY,
+                       const int incpriY, double *carY, const int inccarY);
+void binnedBLAS_dmzasum(const int fold, const int N, const void *X, const int incX,
+                        double *priY, const int incpriY, double *carY, const int inccarY);
+double binnedBLAS_dmzssq(const int fold, const int N, const void *X, const int incX,
+                         const double scaleY, double *priY, const int incpriY, double *carY,
+                         const int inccarY);
+void binnedBLAS_zmzdotu(const int fold, const int N, const void *X, const int incX,
+                        const void *Y, const int incY, double *manZ, const int incmanZ,
+                        double *carZ, const int inccarZ);
+void binnedBLAS_zmzdotc(const int fold, const int N, const void *X, const int incX,
+                        const void *Y, const int incY, double *manZ, const int incmanZ,
+                        double *carZ, const int inccarZ);
+void binnedBLAS_smssum(const int fold, const int N, const float *X, const int incX, float *priY,
+                       const int incpriY, float *carY, const int inccarY);
+void binnedBLAS_smsasum(const int fold, const int N, const float *X, const int incX,
+                        float *priY, const int incpriY, float *carY, const int inccarY);
+float binnedBLAS_smsssq(const int fold, const int N, const float *X, const int incX,
+                        const float scaleY, float *priY, const int incpriY, float *carY,
+                        const int inccarY);
+void binnedBLAS_smsdot(const int fold, const int N, const float *X, const int incX,
+                       const float *Y, const int incY, float *manZ, const int incmanZ,
+                       float *carZ, const int inccarZ);
+void binnedBLAS_cmcsum(const int fold, const int N, const void *X, const int incX, float *priY,
+                       const int incpriY, float *carY, const int inccarY);
+void binnedBLAS_smcasum(const int fold, const int N, const void *X, const int incX,
+                        float *priY, const int incpriY, float *carY, const int inccarY);
+float binnedBLAS_smcssq(const int fold, const int N, const void *X, const int incX,
+                        const float scaleY, float *priY, const int incpriY, float *carY,
+                        const int inccarY);
+void binnedBLAS_cmcdotu(const int fold, const int N, const void *X, const int incX,
+                        const void *Y, const int incY, float *manZ, const int incmanZ,
+                        float *carZ, const int inccarZ);
+void binnedBLAS_cmcdotc(const int fold, const int N, const void *X, const int incX,
+                        const void *Y, const int incY, float *manZ, const int incmanZ,
+                        float *carZ, const int inccarZ);
+
 /* include/binnedBLAS.h:87 (src/binnedBLAS/dbdgemv.ccog:57-162): Y (binned states, stride
  * incY states) += A*fl(alpha*x) or A^T*fl(alpha*x) */
 void binnedBLAS_dbdgemv(const int fold, const char Order, const char TransA, const int M,

@@ -125,6 +125,15 @@ SIGNATURES = {
                                  _c_vp]),
 }
 
+# manual-layout forms: (fold, N, X, incX[, Y, incY][, scale], pri, incpri, car, inccar)
+for _n in ("dmdsum", "dmdasum", "zmzsum", "dmzasum", "smssum", "smsasum", "cmcsum", "smcasum"):
+    SIGNATURES["binnedBLAS_" + _n] = (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp, _c_int, _c_vp, _c_int])
+for _n in ("dmddot", "zmzdotu", "zmzdotc", "smsdot", "cmcdotu", "cmcdotc"):
+    SIGNATURES["binnedBLAS_" + _n] = (None, [_c_int, _c_int, _c_vp, _c_int, _c_vp, _c_int, _c_vp, _c_int,
+                                             _c_vp, _c_int])
+for _n, _r in (("dmdssq", _c_double), ("dmzssq", _c_double), ("smsssq", _c_float), ("smcssq", _c_float)):
+    SIGNATURES["binnedBLAS_" + _n] = (_r, [_c_int, _c_int, _c_vp, _c_int, _r, _c_vp, _c_int, _c_vp, _c_int])
+
 # gemv / gemm of FP32 real (scalars by value) and FP64 / FP32 complex elements (scalars by
 # pointer to two reals), same argument lists as the FP64 forms above
 for _t, _b, _sc in (("s", "sbs", _c_float), ("z", "zbz", _c_vp), ("c", "cbc", _c_vp)):
