@@ -53,3 +53,23 @@ def test_launch_config_validation(rb):
 
 def test_version(rb):
     assert "sm_100a" in rb.version()
+
+
+REF_INCLUDE = "/root/reference/include"   # the ReproBLAS source tree, when present (not on GPU hosts)
+
+
+def test_every_reference_blas_entry_point_is_exported(rb):
+    """Every function include/reproBLAS.h and include/binnedBLAS.h of the reference declare is
+    declared (and, by test_library_exports_header, exported) here under the same name."""
+    import os
+    import re
+    import pytest
+    if not os.path.isdir(REF_INCLUDE):
+        pytest.skip("reference source tree not present")
+    ref = set()
+    for h in ("reproBLAS.h", "binnedBLAS.h"):
+        text = open(os.path.join(REF_INCLUDE, h)).read()
+        ref |= set(re.findall(r"\b((?:reproBLAS|binnedBLAS)_\w+)\s*\(", text))
+    ours = set(rb.exported_symbols())
+    missing = sorted(ref - ours)
+    assert len(ref) >= 100 and not missing, missing
