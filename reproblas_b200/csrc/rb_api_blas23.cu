@@ -97,18 +97,34 @@ bool run_gemv_stream(const GemvReq& q, const Blas23FoldOps* o, Workspace* w, con
   // resident slot (every CTA gets at least one stage). Take the smallest G for which the
   // last CTA of a cut unit merges at most about 4 parts per thread.
   const long long gmax = (long long)di.sms * (nt ? rows_per_sm : cols_per_sm);
-  int G = 2;
-  long long nunits = 0, nb = 0, T = 0, grid = 0;
-  for (;;) {
+  long long nunits = 0, nb = 0, T = 0, grid = 0, parts = 0;
+  auto shape = [&](int G) {
     const long long P = 512 / G;
     nunits = (nout + P - 1) / P;
     nb = nt ? (nred + 16 * G - 1) / (16 * G) : (nred + 8 * G - 1) / (8 * G);
     T = nunits * nb;
     grid = T < gmax ? T : gmax;
     // a unit meets at most ceil((nb-1) / min_range) + 1 CTA ranges, min_range = floor(T/grid)
-    const long long parts = nb / (T / grid) + 2;
+    parts = nb / (T / grid) + 2;
+  };
+  int G = 2;
+  for (;;) {
+    shape(G);
     if ((parts + G - 1) / G <= 4 || G == 8) break;
     G *= 2;
+  }
+  // rows: G = 4 measured as fast or faster than the rule above on every band shape tried
+  // (2048^2 to 16384^2, 1024 x 16384 to 32768 x 4096), as long as its final merge stays within
+  // about 8 parts per thread
+  if (nt && G != 4) {
+    const int g0 = G;
+    shape(4);
+    if ((parts + 3) / 4 <= 8) {
+      G = 4;
+    } else {
+      G = g0;
+      shape(G);
+    }
   }
   g.groups = G;
   g.kslots = nb / (T / grid) + 2;
