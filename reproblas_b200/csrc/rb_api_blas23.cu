@@ -93,7 +93,7 @@ bool run_gemv_stream(const GemvReq& q, const Blas23FoldOps* o, Workspace* w, con
   g.R = Rs;
   g.C = Cs;
   // G thread groups per output (2, 4 or 8): units are bands of P = 512/G rows (stages of
-  // 16G columns) or blocks of P columns (stages of 8G rows), split evenly over one CTA per
+  // 16G columns) or blocks of P columns (stages of 16G rows), split evenly over one CTA per
   // resident slot (every CTA gets at least one stage). Take the smallest G for which the
   // last CTA of a cut unit merges at most about 4 parts per thread.
   const long long gmax = (long long)di.sms * (nt ? rows_per_sm : cols_per_sm);
@@ -101,7 +101,7 @@ bool run_gemv_stream(const GemvReq& q, const Blas23FoldOps* o, Workspace* w, con
   auto shape = [&](int G) {
     const long long P = 512 / G;
     nunits = (nout + P - 1) / P;
-    nb = nt ? (nred + 16 * G - 1) / (16 * G) : (nred + 8 * G - 1) / (8 * G);
+    nb = (nred + 16 * G - 1) / (16 * G);   // stages of 16G columns (rows) / 16G rows (cols)
     T = nunits * nb;
     grid = T < gmax ? T : gmax;
     // a unit meets at most ceil((nb-1) / min_range) + 1 CTA ranges, min_range = floor(T/grid)
@@ -161,18 +161,17 @@ bool run_gemv_stream(const GemvReq& q, const Blas23FoldOps* o, Workspace* w, con
   CUtensorMap tm, tmx;
   cuuint64_t dims[2] = {(cuuint64_t)Cs, (cuuint64_t)Rs};
   cuuint64_t strides[1] = {(cuuint64_t)q.lda * 8};
-  // rows kernel: boxes of 16 columns x P rows, 128-byte swizzle; cols kernel: P x 8G
+  // rows kernel: boxes of 16 columns x P rows, 128-byte swizzle; cols kernel: P x 16G
   const cuuint32_t P = 512u / (cuuint32_t)G;
-  cuuint32_t box[2] = {nt ? 16u : P, nt ? P : 8u * (cuuint32_t)G};
+  cuuint32_t box[2] = {nt ? 16u : P, nt ? P : 16u * (cuuint32_t)G};
   cuuint32_t estr[2] = {1u, 1u};
   CUresult r = enc(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void*)dA, dims, strides, box, estr,
                    CU_TENSOR_MAP_INTERLEAVE_NONE,
                    nt ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  // x (or bx): boxes of one stage's 16G (rows kernel) or 8G (cols kernel) entries (a rank-1
-  // map reads no stride)
+  // x (or bx): boxes of one stage's 16G entries (a rank-1 map reads no stride)
   cuuint64_t xdims[1] = {(cuuint64_t)nred};
-  cuuint32_t xbox[1] = {nt ? 16u * (cuuint32_t)G : 8u * (cuuint32_t)G};
+  cuuint32_t xbox[1] = {16u * (cuuint32_t)G};
   if (r == CUDA_SUCCESS)
     r = enc(&tmx, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 1, (void*)(x_direct ? dX : bx), xdims, strides,
             xbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,

@@ -54,11 +54,13 @@ constexpr uint32_t kRowStageA = kConsumers * 128;        // G boxes of P x 16 do
 constexpr uint32_t kRowStageBytes = kRowStageA + 1024;  // + up to 128 x, 1 KB aligned
 template <int F> __host__ __device__ constexpr int row_stages() { return 3; }
 // Column reduction (out_c = sum_r A_rc bx_r): units are blocks of P columns. A stage is one
-// box of 8G rows x P columns (32 KB, no swizzle) and the 8G matching x; group q takes rows
-// q, q+G, ..., q+7G of it (even and odd ones into two accumulators).
-constexpr uint32_t kColStageA = kConsumers * 64;         // 32 KB
-constexpr uint32_t kColStageBytes = kColStageA + 512;   // + up to 64 x
-template <int F> __host__ __device__ constexpr int col_stages() { return 6; }
+// box of 16G rows x P columns (64 KB, no swizzle) and the 16G matching x; group q takes rows
+// q, q+G, ..., q+15G of it (even and odd ones into two accumulators), 16 elements per thread
+// per stage like the row reduction.
+constexpr int kColRowsPerGroup = 16;
+constexpr uint32_t kColStageA = kConsumers * 128;        // 64 KB
+constexpr uint32_t kColStageBytes = kColStageA + 1024;  // + up to 128 x
+template <int F> __host__ __device__ constexpr int col_stages() { return 3; }
 
 template <int F>
 __host__ __device__ constexpr size_t tree_bytes() { return (size_t)(2 * F + 1) * kConsumers * 8; }
@@ -398,7 +400,7 @@ gemv_rows_stream_kernel(StreamArgs g, const __grid_constant__ CUtensorMap tm,
 }
 
 // ---------------------------------------------------------------------------------------
-// Column reduction: units are blocks of P = 512/G columns, nb = ceil(R / 8G) stages each.
+// Column reduction: units are blocks of P = 512/G columns, nb = ceil(R / 16G) stages each.
 // ---------------------------------------------------------------------------------------
 template <int F>
 __global__ void __launch_bounds__(kThreads, 1)
@@ -414,7 +416,7 @@ gemv_cols_stream_kernel(StreamArgs g, const __grid_constant__ CUtensorMap tm,
   double* tsm = (double*)(ring + (size_t)NST * kColStageBytes);
   const int tid = threadIdx.x, lane = tid & 31;
   const int G = g.groups, P = kConsumers / G, lgP = __ffs(P) - 1;
-  const int RS = 8 * G;                                  // rows per stage
+  const int RS = kColRowsPerGroup * G;                   // rows per stage
   const int grp = tid >> lgP, p = tid & (P - 1);
   const long long nb = (g.R + RS - 1) / RS;
   const Split sp((g.C + P - 1) / P, nb);
@@ -452,19 +454,22 @@ gemv_cols_stream_kernel(StreamArgs g, const __grid_constant__ CUtensorMap tm,
       if (stage_ready(full, r, &abort_flag)) {
         const double* As = (const double*)(ring + (size_t)r.st * kColStageBytes);
         const double* xs = (const double*)((const unsigned char*)As + kColStageA);
-        double ve[4], vo[4];
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-          const int r0 = grp + G * 2 * k, r1 = r0 + G;
-          double x0 = xs[r0], x1 = xs[r1];
-          if (g.scale_x) {
-            x0 = __dmul_rn(x0, g.alpha);
-            x1 = __dmul_rn(x1, g.alpha);
+        for (int h = 0; h < 2; h++) {
+          double ve[4], vo[4];
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            const int r0 = grp + G * (8 * h + 2 * k), r1 = r0 + G;
+            double x0 = xs[r0], x1 = xs[r1];
+            if (g.scale_x) {
+              x0 = __dmul_rn(x0, g.alpha);
+              x1 = __dmul_rn(x1, g.alpha);
+            }
+            ve[k] = __dmul_rn(As[r0 * P + p], x0);
+            vo[k] = __dmul_rn(As[r1 * P + p], x1);
           }
-          ve[k] = __dmul_rn(As[r0 * P + p], x0);
-          vo[k] = __dmul_rn(As[r1 * P + p], x1);
+          tile2<double, F, 4>(a0, ve, a1, vo);
         }
-        tile2<double, F, 4>(a0, ve, a1, vo);
       } else {
         lost = true;
       }
