@@ -75,6 +75,23 @@ template <> __device__ __forceinline__ float scale_of_key<float>(unsigned key) {
 __device__ __forceinline__ double bdiv(double a, double b) { return __ddiv_rn(a, b); }
 __device__ __forceinline__ float bdiv(float a, float b) { return __fdiv_rn(a, b); }
 
+// 1/s. The scales are powers of two: for a positive normal 2^k whose reciprocal 2^-k is normal
+// too, that reciprocal is the exponent field mirrored (exactly the quotient); any other value
+// (a caller's scale need not be a power of two) takes the division.
+__device__ __forceinline__ double recip_scale(double s) {
+  const unsigned long long u = (unsigned long long)__double_as_longlong(s);
+  const unsigned long long e = u >> 52;   // includes the sign bit: negative values fail below
+  if ((u & 0x000fffffffffffffull) == 0 && e >= 1 && e <= 2045)
+    return __longlong_as_double((long long)((2046ull - e) << 52));
+  return __ddiv_rn(1.0, s);
+}
+__device__ __forceinline__ float recip_scale(float s) {
+  const unsigned u = __float_as_uint(s);
+  const unsigned e = u >> 23;
+  if ((u & 0x007fffffu) == 0 && e >= 1 && e <= 253) return __uint_as_float((254u - e) << 23);
+  return __fdiv_rn(1.0f, s);
+}
+
 template <typename T, int F>
 __device__ __forceinline__ void rescale(Acc<T, F>& a, T x, T scaleY) {
   using B = BT<T>;
@@ -178,7 +195,7 @@ struct Red1 {
     // FP32: 1/scl kept between tiles (the division dominated the FP32 tile); FP64 recomputes
     // it, which keeps the FP64 kernel's registers within its 4-CTA budget
     if (sizeof(T) == 8 || inv_of != scl) {
-      inv = bdiv(T(1), (T)scl);
+      inv = recip_scale((T)scl);
       inv_of = scl;
     }
     T v[K];
