@@ -120,12 +120,12 @@ def _oracle_merge_kind(kind, reverse):
         order = range(count - 1, -1, -1) if reverse else range(count)
         for i in order:
             rec = np.ascontiguousarray(g[i * n:(i + 1) * n])
-            if kind == "z":
-                P.zbzbadd(fold, ptr(rec), ptr(o))
-            elif kind == "dsq":
+            if kind in ("z", "c", "s"):
+                getattr(P, {"z": "zbzbadd", "c": "cbcbadd", "s": "sbsbadd"}[kind])(fold, ptr(rec), ptr(o))
+            elif kind in ("dsq", "ssq"):
                 body = o[1:].copy()
-                o[0] = P.dbdbaddsq(fold, float(rec[0]), ptr(np.ascontiguousarray(rec[1:])), float(o[0]),
-                                   ptr(body))
+                add = P.dbdbaddsq if kind == "dsq" else P.sbsbaddsq
+                o[0] = add(fold, float(rec[0]), ptr(np.ascontiguousarray(rec[1:])), float(o[0]), ptr(body))
                 o[1:] = body
     return merge
 
@@ -207,3 +207,74 @@ def test_record_lengths_and_kind_check():
         rbdist.allgather_merge(torch.zeros(5), 3, kind="d")
     with pytest.raises(ValueError):
         rbdist.allgather_merge(torch.zeros(6), 3, kind="q")
+
+
+def _fp32_worker(rank, world, port, n, fold, q):
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import torch.distributed as dist
+    from _ffi import port as oport, ptr, binned_zeros
+    from _data import gen, gen_complex
+    rbdist = _load_rbdist()
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        P = oport()
+        start, length = rbdist.shard(n, rank, world)
+        out = {}
+        xs = gen("normal", n, 11, np.float32)
+        st = binned_zeros(fold, "s")
+        P.sbssum(fold, length, ptr(xs[start:]), 1, ptr(st))
+        xc, yc = gen_complex("normal", n, 12, np.complex64), gen_complex("normal", n, 13, np.complex64)
+        stc = binned_zeros(fold, "c")
+        P.cbcdotu(fold, length, ptr(xc[start:]), 1, ptr(yc[start:]), 1, ptr(stc))
+        v = gen("loguniform", n, 14, np.float32)
+        rec = np.zeros(1 + 2 * fold, np.float32)
+        body = binned_zeros(fold, "s")
+        rec[0] = P.sbsssq(fold, length, ptr(v[start:]), 1, 0.0, ptr(body))
+        rec[1:] = body
+        for rev in (False, True):
+            for kind, state in (("s", st), ("c", stc), ("ssq", rec)):
+                m = rbdist.allgather_merge(torch.from_numpy(state), fold, kind=kind,
+                                           merge=_oracle_merge_kind(kind, rev))
+                out[(kind, rev)] = m.numpy().tobytes()
+        q.put((rank, out))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_allgather_merge_fp32_kinds():
+    """float, float complex and scaled FP32 records through the exchange with 2 ranks."""
+    from _ffi import port, ptr, binned_zeros
+    from _data import gen, gen_complex
+    n, fold, world = 40009, 3, 2
+    P = port()
+    want = {}
+    xs = gen("normal", n, 11, np.float32)
+    st = binned_zeros(fold, "s")
+    P.sbssum(fold, n, ptr(xs), 1, ptr(st))
+    want["s"] = st.tobytes()
+    xc, yc = gen_complex("normal", n, 12, np.complex64), gen_complex("normal", n, 13, np.complex64)
+    stc = binned_zeros(fold, "c")
+    P.cbcdotu(fold, n, ptr(xc), 1, ptr(yc), 1, ptr(stc))
+    want["c"] = stc.tobytes()
+    v = gen("loguniform", n, 14, np.float32)
+    rec = np.zeros(1 + 2 * fold, np.float32)
+    body = binned_zeros(fold, "s")
+    rec[0] = P.sbsssq(fold, n, ptr(v), 1, 0.0, ptr(body))
+    rec[1:] = body
+    want["ssq"] = rec.tobytes()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    p = _free_port()
+    procs = [ctx.Process(target=_fp32_worker, args=(r, world, p, n, fold, q)) for r in range(world)]
+    for pr in procs:
+        pr.start()
+    got = [q.get(timeout=120) for _ in range(world)]
+    for pr in procs:
+        pr.join(timeout=60)
+        assert pr.exitcode == 0
+    for rank, out in got:
+        for (kind, rev), b in out.items():
+            assert b == want[kind], (rank, kind, rev)
