@@ -580,7 +580,7 @@ def secondary(args):
     except Exception:
         peak_bf16 = 1590.0
     rng = np.random.default_rng(8192)
-    # plain binned dgemm, BASELINE configuration: M=N=K=2048, uniform(-1,1), alpha 1.5, beta 0.5
+    # plain binned dgemm, the reference benchmark shape: M=N=K=2048, uniform(-1,1), alpha 1.5, beta 0.5
     n = 2048
     A = torch.from_numpy(rng.uniform(-1, 1, (n, n))).cuda()
     B = torch.from_numpy(rng.uniform(-1, 1, (n, n))).cuda()
