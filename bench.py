@@ -175,6 +175,29 @@ def cpu_reference_dot(R, x, y, threads):
     return dt, total
 
 
+def workload_config(log2n):
+    """The workload's config (identical in both arms)."""
+    n = 1 << log2n
+    return {"workload": "reproBLAS_ddot fold 3, N=2^%d FP64 per GPU" % log2n,
+            "n_per_gpu": n, "fold": FOLD, "l2": "inputs 4 GiB >> 126 MB L2, no flush",
+            "parallelism": "weak: shard per GPU, NCCL all-gather of 48-byte states"}
+
+
+def cpu_reference_rddot_1core(R, x, y, reps):
+    """The reference's reproBLAS_rddot exactly as shipped (single-threaded): best time of
+    `reps` calls after one warm-up call, and the result."""
+    from _ffi import ptr
+    n = len(x)
+    res = R.rddot(FOLD, n, ptr(x), 1, ptr(y), 1)
+    best = None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        res = R.rddot(FOLD, n, ptr(x), 1, ptr(y), 1)
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    return best, res
+
+
 def reference_arm(args, rank):
     from _ffi import ref
     if rank != 0:
@@ -190,19 +213,19 @@ def reference_arm(args, rank):
     for _ in range(max(1, min(args.warmup, 2))):
         cpu_reference_dot(R, x, y, threads)
     times = [cpu_reference_dot(R, x, y, threads)[0] for _ in range(args.steps)]
-    t = statistics.mean(times)
+    t = min(times)
     gbs = 16.0 * n / t / 1e9
     print(json.dumps({
         "metric": METRIC, "value": round(gbs, 3), "unit": "GB/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(t * 1e3, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic uniform(-1,1), seed 2024",
-        "config": {"workload": "reproBLAS_ddot fold 3, N=2^%d FP64 (binnedBLAS_dbddot per "
-                               "thread chunk + binned_dbdbadd merge)" % args.log2n,
-                   "n": n, "fold": FOLD},
+        "config": workload_config(args.log2n),
         "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": threads,
                          "kind": "reference",
-                         "sample": "full workload, %d threads, mean of %d steps" % (threads, args.steps)},
+                         "sample": "full workload; %d threads each calling binnedBLAS_dbddot on a "
+                                   "contiguous chunk, merged with binned_dbdbadd; best of %d steps"
+                                   % (threads, args.steps)},
         "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }))
@@ -315,15 +338,20 @@ def ours_arm(args, rank, world, local_rank):
         cpu_reference_dot(R, x[: 1 << 20], y[: 1 << 20], threads)   # warm-up
         times = []
         state = None
-        for _ in range(3):
+        for _ in range(5):
             dt, state = cpu_reference_dot(R, x, y, threads)
             times.append(dt)
         cpu_gbs = 16.0 * n / min(times) / 1e9
         bit_identical = bool(state.tobytes() == gpu_state.tobytes())
+        t1, r1 = cpu_reference_rddot_1core(R, x, y, 5)
         cpu = {"value": round(cpu_gbs, 3), "unit": "GB/s", "cores": threads, "kind": kind,
                "sample": "full N=2^%d workload, %d threads (contiguous chunks + binned_dbdbadd), "
-                         "best of 3" % (args.log2n, threads),
-               "bit_identical_to_gpu": bit_identical}
+                         "best of 5" % (args.log2n, threads),
+               "bit_identical_to_gpu": bit_identical,
+               "one_core": {"value": round(16.0 * n / t1 / 1e9, 3), "unit": "GB/s", "cores": 1,
+                            "api": "reproBLAS_rddot as shipped (single-threaded), best of 5",
+                            "ms": round(t1 * 1e3, 2),
+                            "result_equals_gpu": bool(res is None or r1 == res)}}
 
     sec = None
     if rank == 0 and world == 1 and not args.no_secondary:
@@ -339,10 +367,7 @@ def ours_arm(args, rank, world, local_rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic uniform(-1,1), seed 2024+rank (host-generated)",
-        "config": {"workload": "reproBLAS_ddot fold 3, N=2^%d FP64 per GPU (binnedBLAS_dbddot, "
-                               "device-resident inputs)" % args.log2n,
-                   "n_per_gpu": n, "fold": FOLD, "l2": "inputs 4 GiB >> 126 MB L2, no flush",
-                   "parallelism": "weak: shard per GPU, NCCL all-gather of 48-byte states"},
+        "config": workload_config(args.log2n),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
                      "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
@@ -357,6 +382,9 @@ def ours_arm(args, rank, world, local_rank):
         "cpu_baseline": cpu,
         "result": res,
         "secondary": sec,
+        # last on the line: the compact second half of the headline metric (dgemm plain vs
+        # int8-sliced) and the dgemv fractions
+        "headline": headline(sec),
     }
     traffic = os.path.join(ROOT, "profiles", "ddot_traffic.json")
     if os.path.exists(traffic):
@@ -366,6 +394,30 @@ def ours_arm(args, rank, world, local_rank):
         except Exception:
             pass
     print(json.dumps(line))
+
+
+def headline(sec):
+    """dgemm TFLOP/s (plain binned vs int8-sliced, with error over binned_dbbound) and the
+    dgemv fractions of the HBM peak, compact."""
+    if not sec:
+        return None
+    h = {"dgemm_plain_tflops": {k: sec[k]["tflops"] for k in ("dgemm_plain_2048", "dgemm_plain_8192")
+                                if k in sec}}
+    i8 = {}
+    for S in (6, 7, 8, 10):
+        r = sec.get("dgemm_int8_8192_s%d" % S)
+        if r:
+            i8["s%d" % S] = [r["tflops_effective"], r["speedup_vs_plain"], r["int8_frac"],
+                             float("%.3g" % r["err_over_binned_bound_max"])]
+    h["dgemm_int8_8192"] = i8
+    h["dgemm_int8_fields"] = "[effective TFLOP/s, x plain 8192, int8 frac, max err/dbbound]"
+    h["dgemv_frac"] = {k[6:]: v["frac_of_copy_peak"] for k, v in sec.items()
+                       if k.startswith("dgemv_")}
+    b = sec.get("batched")
+    if b:
+        h["batched_ms"] = [b["ms"], b["segments_only_ms"], b["gemms_only_ms"],
+                           b["spot_check_bit_identical"]]
+    return h
 
 
 def _event_time(torch, fn, reps, warm=1):

@@ -38,10 +38,15 @@
 extern "C" {
 #endif
 
+/* The binned types of the reference. When its binned.h is included first (include guard
+ * BINNED_H_), its identical typedefs are used; include binned.h before this header when a
+ * translation unit needs both (C99 warns about a repeated typedef, C11 accepts it). */
+#ifndef BINNED_H_
 typedef double double_binned;          /* include/binned.h:46 */
 typedef double double_complex_binned;  /* include/binned.h:55 */
 typedef float float_binned;            /* include/binned.h:64 */
 typedef float float_complex_binned;    /* include/binned.h:73 */
+#endif
 
 /* ------------------------------------------------------------------------------------
  * reproBLAS level (value-returning; temporaries are internal). include/reproBLAS.h
@@ -534,12 +539,16 @@ int rb_sbsbaddsq_states(const int fold, const int count, const float *states, fl
  * memory; Z (a device double_binned, accumulated into as by binnedBLAS_dbddot) and result
  * (a device double receiving the converted sum) may each be NULL. Work is enqueued on
  * `stream` (a cudaStream_t; NULL = legacy default stream) and not waited for.
+ * Z and result must be 8-byte aligned.
  * Scratch: a fixed 128 KiB device array inside this library, one per GPU that loads it,
  * held until exit; it holds (128 KiB - 256 B) / ((2*fold + 2) * 8 B) CTA records, and a
  * launch shape needing more (see rb_set_launch_config) is rejected with
- * RB_ERR_INVALID_ARG. The first call on each device looks the array's address up
- * (cudaGetSymbolAddress); make it before any stream capture. All calls share the array:
- * calls that overlap on the GPU race and must be serialised by the caller.
+ * RB_ERR_INVALID_ARG. The first call on each device (and in each new CUDA context, e.g.
+ * after cudaDeviceReset) looks the array's address up (cudaGetSymbolAddress). Under the
+ * default lazy module loading the first call on a device, and the first at each fold, may
+ * also load this library's device code, for which the driver allocates memory: make those
+ * calls during set-up, before any stream capture. All calls share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller.
  * Returns an RB_* code. */
 int rb_ddot_noalloc(const int fold, const int N, const double *X, const int incX,
                     const double *Y, const int incY, double_binned *Z, double *result,

@@ -12,7 +12,11 @@
 // driver places when it loads this library's device code; every GPU that loads the
 // library holds it until the process exits. Host code cannot use the array's name as a
 // device address, so the first call on each device (with that device current) looks the
-// address up with cudaGetSymbolAddress and caches it; make that first call before any
+// address up with cudaGetSymbolAddress and caches it together with the CUDA context it
+// belongs to; a call from another context (after cudaDeviceReset, or under a context the
+// caller made current with the driver API) looks it up again. With the default lazy module
+// loading, that first call on a device, and the first at each fold, may also load device
+// code, which the driver allocates memory for: make those calls during set-up, before any
 // stream capture. The ticket is cleared with cudaMemsetAsync before every launch (a clear
 // of existing memory, not an allocation).
 //
@@ -34,12 +38,36 @@ namespace {
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
-void* g_scratch_addr[kMaxDevices] = {};
+struct ScratchSlot {
+  CUcontext ctx = nullptr;   // context the address was looked up in
+  void* addr = nullptr;
+};
+ScratchSlot g_scratch[kMaxDevices];
 
-// Device address of g_noalloc_scratch on the current device (looked up once per device).
+// The calling thread's current CUDA context (through the runtime's driver entry point, so
+// the library needs no libcuda link), or nullptr when none is current or the query fails.
+CUcontext current_context() {
+  static PFN_cuCtxGetCurrent_v4000 get = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get = (PFN_cuCtxGetCurrent_v4000)p;
+  });
+  CUcontext c = nullptr;
+  if (!get || get(&c) != CUDA_SUCCESS) return nullptr;
+  return c;
+}
+
+// Device address of g_noalloc_scratch on the current device, looked up once per device and
+// context (the lookup also makes the device's primary context current when none is).
 void* scratch_address(int dev) {
   std::lock_guard<std::mutex> g(g_setup_mu);
-  if (!g_scratch_addr[dev]) {
+  CUcontext ctx = current_context();
+  ScratchSlot& slot = g_scratch[dev];
+  if (!slot.addr || !ctx || slot.ctx != ctx) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || p == nullptr) {
@@ -47,9 +75,10 @@ void* scratch_address(int dev) {
                                  cudaGetErrorString(e));
       return nullptr;
     }
-    g_scratch_addr[dev] = p;
+    slot.addr = p;
+    slot.ctx = current_context();
   }
-  return g_scratch_addr[dev];
+  return slot.addr;
 }
 
 }  // namespace
@@ -74,8 +103,10 @@ extern "C" int rb_ddot_noalloc(const int fold, const int N, const double* X, con
                                   "memory (host inputs would need staging buffers)");
     return RB_ERR_INVALID_ARG;
   }
-  if ((Z && !on_device(Z)) || (result && !on_device(result))) {
-    set_error(RB_ERR_INVALID_ARG, "rb_ddot_noalloc: Z and result must be device memory or NULL");
+  if ((Z && (!on_device(Z) || ((uintptr_t)Z % 8) != 0)) ||
+      (result && (!on_device(result) || ((uintptr_t)result % 8) != 0))) {
+    set_error(RB_ERR_INVALID_ARG, "rb_ddot_noalloc: Z and result must be 8-byte aligned "
+                                  "device memory or NULL");
     return RB_ERR_INVALID_ARG;
   }
   int dev = 0;

@@ -11,6 +11,17 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PORT_SO = os.path.join(ROOT, "oracle", "_build", "librb_oracle.so")
 REF_SO = os.path.join(ROOT, "oracle", "_ref", "libreproblas_ref.so")
+REF_SOURCE_NOTE = os.path.join(ROOT, "oracle", "_ref", "SOURCE")
+
+
+def reference_tree():
+    """The ReproBLAS source tree, or None: $REPROBLAS_SRC, else the tree oracle/_ref was
+    compiled from (the build records it in oracle/_ref/SOURCE), when it exists here."""
+    cand = os.environ.get("REPROBLAS_SRC")
+    if not cand and os.path.exists(REF_SOURCE_NOTE):
+        with open(REF_SOURCE_NOTE) as f:
+            cand = f.read().strip()
+    return cand if cand and os.path.isdir(cand) else None
 
 c_int, c_double, c_float, c_char, c_vp = (ctypes.c_int, ctypes.c_double, ctypes.c_float,
                                           ctypes.c_char, ctypes.c_void_p)
@@ -77,6 +88,7 @@ _SIGS = {
     "dbdbadd": (None, [c_int, c_vp, c_vp]),
     "dbdconv": (None, [c_int, c_double, c_vp]),
     "ddbconv": (c_double, [c_int, c_vp]),
+    "ddmconv": (c_double, [c_int, c_vp, c_int, c_vp, c_int]),
     "dbdbaddsq": (c_double, [c_int, c_double, c_vp, c_double, c_vp]),
     "dbbound": (c_double, [c_int, c_int, c_double, c_double]),
     "dscale": (c_double, [c_double]),
@@ -126,7 +138,7 @@ _REF_NAMES = {
     "camax_sub": "binnedBLAS_camax_sub", "zamaxm_sub": "binnedBLAS_zamaxm_sub",
     "camaxm_sub": "binnedBLAS_camaxm_sub",
     "rsnrm2": "reproBLAS_rsnrm2", "rdznrm2": "reproBLAS_rdznrm2", "rscnrm2": "reproBLAS_rscnrm2",
-    "dbdbadd": "binned_dbdbadd", "dbdconv": "binned_dbdconv", "ddbconv": "binned_ddbconv",
+    "dbdbadd": "binned_dbdbadd", "dbdconv": "binned_dbdconv", "ddbconv": "binned_ddbconv", "ddmconv": "binned_ddmconv",
     "dbdbaddsq": "binned_dbdbaddsq", "dbbound": "binned_dbbound", "dscale": "binned_dscale",
     "dindex": "binned_dindex", "sindex": "binned_sindex", "sbsbadd": "binned_sbsbadd",
     "ssbconv": "binned_ssbconv",
@@ -163,7 +175,34 @@ def port():
         extra.restype = c_double
         extra.argtypes = [c_int, c_vp, c_int, c_vp, c_int]
         _port.exact_dot = extra
+        for nm in ("rbo_fill_d", "rbo_fill_s"):
+            fn = getattr(_port.lib, nm)
+            fn.restype = c_int
+            fn.argtypes = [c_int, ctypes.c_ulonglong, ctypes.c_longlong, c_vp, c_int, c_int]
+        _port.fill_d = _port.lib.rbo_fill_d
+        _port.fill_s = _port.lib.rbo_fill_s
     return _port
+
+
+FILL_DISTS = {"uniform": 0, "normal": 1, "loguniform": 2, "illcond": 3}
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def fill(dist, seed, n, dtype=np.float64, unit=1, out=None):
+    """A seeded vector of n values of the given distribution (oracle/rb_fill.c): element i
+    depends only on (dist, seed, i), so prefixes of a long vector are the shorter vectors.
+    `unit` = 2 builds the ill-conditioned pairs from complex items (z, -z)."""
+    out = np.empty(n, dtype) if out is None else out
+    f = port().fill_d if out.dtype == np.float64 else port().fill_s
+    rc = f(FILL_DISTS[dist], seed, n, out.ctypes.data, unit, min(64, host_threads()))
+    assert rc == 0
+    return out
 
 
 def ref():

@@ -55,17 +55,17 @@ def test_version(rb):
     assert "sm_100a" in rb.version()
 
 
-REF_INCLUDE = "/root/reference/include"   # the ReproBLAS source tree, when present (not on GPU hosts)
-
-
 def test_every_reference_blas_entry_point_is_exported(rb):
     """Every function include/reproBLAS.h and include/binnedBLAS.h of the reference declare is
     declared (and, by test_library_exports_header, exported) here under the same name."""
     import os
     import re
     import pytest
-    if not os.path.isdir(REF_INCLUDE):
+    from _ffi import reference_tree
+    tree = reference_tree()
+    if tree is None:
         pytest.skip("reference source tree not present")
+    REF_INCLUDE = os.path.join(tree, "include")
     ref = set()
     for h in ("reproBLAS.h", "binnedBLAS.h"):
         text = open(os.path.join(REF_INCLUDE, h)).read()

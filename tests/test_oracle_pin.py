@@ -17,7 +17,7 @@ import pytest
 
 from _cmp import from_hex, same_bits, same_state, same_value
 from _data import gen, gen_complex, blas23_operands
-from _ffi import binned_zeros, ptr, ref
+from _ffi import binned_zeros, ptr, ref, reference_tree
 import hashlib
 
 
@@ -144,7 +144,7 @@ def test_port_matches_reference_special_values(port):
         assert same_value(a, b)
 
 
-REF_DATA = "/root/reference/tests/checks/data"
+REF_DATA = os.path.join(reference_tree() or "/nonexistent", "tests", "checks", "data")
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_DATA), reason="ReproBLAS tree not present")
