@@ -505,6 +505,25 @@ void rb_set_launch_config(int ctas_per_sm, int threads_per_cta);
 /* Number of kernels this library launched since load (all threads). */
 unsigned long long rb_kernel_launch_count(void);
 
+/* Waits for the calling thread's current stream and reports what its asynchronous calls
+ * could not: RB_ERR_CUDA if a kernel's bounded pipeline wait gave up since the last report
+ * (the TMA-fed dgemv kernels mark the entries they could not finish NaN; calls that wait
+ * for their stream report it themselves), or a CUDA error of the stream. No reference
+ * counterpart (the reference is synchronous). */
+int rb_synchronize(void);
+
+/* Failure-path test hooks (process-wide; no reference counterpart). They exist so that the
+ * error paths can be exercised without a real fault.
+ * rb_debug_fail_allocations(n): the next n device or pinned allocations of the library's
+ * workspaces fail as on an exhausted device (RB_ERR_ALLOC); 0 turns it off.
+ * rb_debug_pipeline_fault(stop_after, wait_polls): the TMA producers of the dgemv and
+ * int8-sliced dgemm kernels issue at most `stop_after` stages per CTA (< 0: all), and the
+ * threads waiting for a stage's data give up after `wait_polls` polls (0: the default
+ * ~2 s); waits for copies or tensor-core work already issued keep the default limit, so
+ * no CTA exits with either in flight. (-1, 0) turns it off. */
+void rb_debug_fail_allocations(int count);
+void rb_debug_pipeline_fault(long long stop_after, long long wait_polls);
+
 /* out += states[0] + ... + states[count-1], all fold-`fold` double_binned in DEVICE
  * memory, merged on the GPU with the reference's binned_dbdbadd arithmetic (the operation
  * binnedMPI_DBDBADD applies, src/binnedMPI/DBDBADD.ccog:22-24). Enqueued on the current

@@ -191,6 +191,7 @@ bool run_gemv_stream(const GemvReq& q, const Blas23FoldOps* o, Workspace* w, con
   g.scratch = part;
   g.tickets = w->tickets;
   g.status = w->dstatus();
+  pipeline_fault(&g.stop_after, &g.wait_polls);
   if (!x_direct) {
     count_launch();
     long long sgrid = (nred + 255) / 256;

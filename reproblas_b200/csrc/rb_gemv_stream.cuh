@@ -109,14 +109,17 @@ struct Ring {
 
 // Producer (lane 0 of warp 8): per stage, `issue(u, j, dst, fb)` starts the copies of
 // stage j of unit u into shared address dst, all completing on mbarrier fb with TX bytes in
-// total.
+// total. Before returning it waits (bounded) until every copy it issued has landed, so that
+// none is still writing shared memory when the CTA exits, whichever side gave up.
 template <int NST, uint32_t STAGE, class Issue>
 __device__ __forceinline__ void produce(unsigned char* ring, unsigned long long* full,
                                         unsigned long long* empty, int* abort_flag,
-                                        const Split& sp, long long nb, uint32_t TX, Issue issue) {
+                                        const Split& sp, long long nb, uint32_t TX,
+                                        long long stop_after, Issue issue) {
   Ring r;
   long long u = sp.x0 / nb, j = sp.x0 % nb, issued = 0;
   for (long long x = sp.x0; x < sp.x1; x++, issued++) {
+    if (stop_after >= 0 && issued >= stop_after) break;   // test hook: stop feeding the ring
     if (issued >= NST && !mbar_wait_bounded(smem_u32(&empty[r.st]), r.ph ^ 1u)) {
       atomicExch(abort_flag, 1);
       break;
@@ -128,20 +131,18 @@ __device__ __forceinline__ void produce(unsigned char* ring, unsigned long long*
     r.next(NST);
     if (++j == nb) { j = 0; u++; }
   }
-  // on abort, let the copies in flight land (bounded) before the CTA exits
-  if (*(volatile int*)abort_flag) {
-    const long long first = issued > NST ? issued - NST : 0;
-    for (long long k = first; k < issued; k++)
-      mbar_wait_bounded(smem_u32(&full[k % NST]), (unsigned)((k / NST) & 1));
-  }
+  // the last phase of each slot it used belongs to one of the last NST stages it issued
+  const long long first = issued > NST ? issued - NST : 0;
+  for (long long k = first; k < issued; k++)
+    mbar_wait_bounded(smem_u32(&full[k % NST]), (unsigned)((k / NST) & 1));
 }
 
 // Consumer side of one stage: wait for it (unless aborted); false when the data is not
 // there (abort), in which case the caller skips its deposits.
 __device__ __forceinline__ bool stage_ready(unsigned long long* full, const Ring& r,
-                                            int* abort_flag) {
+                                            int* abort_flag, long long polls) {
   if (*(volatile int*)abort_flag) return false;
-  if (!mbar_wait_bounded(smem_u32(&full[r.st]), r.ph)) {
+  if (!mbar_wait_bounded(smem_u32(&full[r.st]), r.ph, polls)) {
     atomicExch(abort_flag, 1);
     return false;
   }
@@ -341,11 +342,12 @@ gemv_rows_stream_kernel(StreamArgs g, const __grid_constant__ CUtensorMap tm,
         tma_load_1d(dst + kRowStageA, tmxp, c, fb);
       };
       produce<NST, kRowStageBytes>(ring, full, empty, &abort_flag, sp, nb,
-                                   kRowStageA + (uint32_t)SC * 8, issue);
+                                   kRowStageA + (uint32_t)SC * 8, g.stop_after, issue);
     }
   } else {
     Ring r;
     Pending pend;
+    const long long polls = g.wait_polls > 0 ? g.wait_polls : kWaitPolls;
     long long u = sp.x0 / nb, j = sp.x0 % nb;
     Acc<double, F> a0, a1;
     a0.zero();
@@ -354,7 +356,7 @@ gemv_rows_stream_kernel(StreamArgs g, const __grid_constant__ CUtensorMap tm,
     const uint32_t rowoff = (uint32_t)grp * (kRowStageA / G) + (uint32_t)p * 128;
     const int sw = p & 7;
     for (long long x = sp.x0; x < sp.x1; x++) {
-      if (stage_ready(full, r, &abort_flag)) {
+      if (stage_ready(full, r, &abort_flag, polls)) {
         const unsigned char* st = ring + (size_t)r.st * kRowStageBytes;
         const double* xs = (const double*)(st + kRowStageA) + grp * kRowBoxC;
 #pragma unroll
@@ -440,18 +442,19 @@ gemv_cols_stream_kernel(StreamArgs g, const __grid_constant__ CUtensorMap tm,
         tma_load_1d(dst + kColStageA, tmxp, (int)(j * RS), fb);
       };
       produce<NST, kColStageBytes>(ring, full, empty, &abort_flag, sp, nb,
-                                          kColStageA + (uint32_t)RS * 8, issue);
+                                   kColStageA + (uint32_t)RS * 8, g.stop_after, issue);
     }
   } else {
     Ring r;
     Pending pend;
+    const long long polls = g.wait_polls > 0 ? g.wait_polls : kWaitPolls;
     long long u = sp.x0 / nb, j = sp.x0 % nb;
     Acc<double, F> a0, a1;
     a0.zero();
     a1.zero();
     bool lost = false;
     for (long long x = sp.x0; x < sp.x1; x++) {
-      if (stage_ready(full, r, &abort_flag)) {
+      if (stage_ready(full, r, &abort_flag, polls)) {
         const double* As = (const double*)(ring + (size_t)r.st * kColStageBytes);
         const double* xs = (const double*)((const unsigned char*)As + kColStageA);
 #pragma unroll

@@ -81,10 +81,16 @@ struct Workspace {
   bool ensure_ring(size_t chunk);
   bool ensure_big(size_t bytes);
   bool ensure_tickets(size_t n);
+  void release();   // frees everything held (a workspace whose set-up failed)
 };
 
-// Locked workspace of the calling thread's current device and stream, or nullptr (error set).
-Workspace* acquire_workspace(std::unique_lock<std::mutex>* lock);
+// Locked workspace of the calling thread's current device and stream, or nullptr (error
+// set); with create = false, nullptr when no call has made one yet.
+Workspace* acquire_workspace(std::unique_lock<std::mutex>* lock, bool create = true);
+
+// cudaMalloc, or a reported cudaErrorMemoryAllocation while the allocation-failure test hook
+// (rb_debug_fail_allocations) has failures left.
+cudaError_t dev_malloc(void** p, size_t bytes);
 
 // Grid size for a reduction over `work` elements with `elems_per_thread` per thread.
 int reduction_grid(long long work, int elems_per_thread, int threads, int occupancy_per_sm);

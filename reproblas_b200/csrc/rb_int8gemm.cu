@@ -167,6 +167,7 @@ int run_int8(const Int8Req& q) {
     g.last_chunk = ch == nchunks - 1;
     g.Cbin = cbin;
     g.status = sa.status;
+    pipeline_fault(&g.stop_after, &g.wait_polls);
     g.raw = (ch == 0) ? q.raw : nullptr;
     CUtensorMap tmA, tmB;
     if (!encode_slices(&tmA, sa.As, Kp, sa.Mp, q.S, i8::BM) ||

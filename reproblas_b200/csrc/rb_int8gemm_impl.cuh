@@ -230,6 +230,11 @@ struct GemmI8Args {
   double* Cbin;                 // [M*N*2F] partial binned states between K chunks
   int* status;                  // 2: a bounded wait timed out
   int* raw;                     // test hook: raw accumulators instead of the epilogue
+  // failure-path test hook (rb_debug_pipeline_fault): the producer issues at most
+  // `stop_after` K steps (< 0: all), and the MMA thread gives up waiting for a stage's data
+  // after `wait_polls` polls (0: the default ~2 s)
+  long long stop_after;
+  long long wait_polls;
 };
 
 template <int S>
@@ -305,6 +310,7 @@ gemm_i8_kernel(GemmI8Args g, const __grid_constant__ CUtensorMap tmA,
     if (lane == 0) {
       int issued = 0;
       for (int it = 0; it < nk; it++) {
+        if (g.stop_after >= 0 && it >= g.stop_after) break;   // test hook: stop feeding the ring
         const int st = it % NST;
         if (it >= NST &&
             !mbar_wait_bounded(smem_u32(&empty_bar[st]), (unsigned)(((it / NST) - 1) & 1))) {
@@ -322,19 +328,20 @@ gemm_i8_kernel(GemmI8Args g, const __grid_constant__ CUtensorMap tmA,
         tma_load_4d(sB, &tmB, 0, (int)(n0 / 8), 0, 2 * it, fb);
         issued = it + 1;
       }
-      // on abort, let this thread's copies in flight land (bounded) before the CTA exits
-      for (int it = (issued > NST ? issued - NST : 0); it < issued && *(volatile int*)&abort_flag; it++)
+      // wait (bounded) until every copy this thread issued has landed, so that none still
+      // writes shared memory when the CTA exits, whichever side gave up: the last phase of
+      // each slot belongs to one of the last NST steps issued
+      for (int it = (issued > NST ? issued - NST : 0); it < issued; it++)
         mbar_wait_bounded(smem_u32(&full_bar[it % NST]), (unsigned)((it / NST) & 1));
     }
   } else if (warp == 9) {
     // ---- MMA issuer ----
     if (lane == 0) {
-      bool ok = true;
+      const long long polls = g.wait_polls > 0 ? g.wait_polls : kWaitPolls;
       for (int it = 0; it < nk; it++) {
         const int st = it % NST;
-        if (!mbar_wait_bounded(smem_u32(&full_bar[st]), (unsigned)((it / NST) & 1))) {
+        if (!mbar_wait_bounded(smem_u32(&full_bar[st]), (unsigned)((it / NST) & 1), polls)) {
           atomicExch(&abort_flag, 1);
-          ok = false;
           break;
         }
         tc_fence_after();
@@ -355,7 +362,9 @@ gemm_i8_kernel(GemmI8Args g, const __grid_constant__ CUtensorMap tmA,
         }
         mma_commit(smem_u32(&empty_bar[st]));   // frees the stage when these MMAs finish
       }
-      if (ok) mma_commit(smem_u32(&done_bar));
+      // done_bar completes once every MMA this thread issued has finished, also after a
+      // wait gave up: the epilogue reads TMEM, and the CTA frees it, only after that
+      mma_commit(smem_u32(&done_bar));
     }
   } else {
     // ---- epilogue warps 0-7: wait for the accumulators ----
@@ -365,6 +374,23 @@ gemm_i8_kernel(GemmI8Args g, const __grid_constant__ CUtensorMap tmA,
   tc_fence_after();
   const bool ok = abort_flag == 0;
   if (!ok && tid == 0) atomicExch(g.status, 2);
+  if (!ok && warp < 8 && !g.raw) {
+    // the tile's entries come out NaN: C itself in the last K chunk, else a NaN state that
+    // the following chunks carry into C
+    const long long row = m0 + (warp & 3) * 32 + lane;
+    const double nan = __longlong_as_double(0x7ff8000000000000ll);
+    const int c0 = (warp >> 2) * (BN / 2);
+    for (int c = c0; row < g.M && c < c0 + BN / 2 && n0 + c < g.N; c++) {
+      const long long col = n0 + c;
+      if (g.last_chunk) {
+        g.C[row * g.sci + col * g.scj] = nan;
+      } else {
+        double* sp = g.Cbin + (row * g.N + col) * 2 * F;
+        sp[0] = nan;
+        for (int i = 1; i < 2 * F; i++) sp[i] = 0.0;
+      }
+    }
+  }
 
   // ---- epilogue: warp w reads TMEM lanes 32(w%4)..+31 (rows m0 + 32(w%4) + lane) and the
   // columns of half w/4 of the tile ----

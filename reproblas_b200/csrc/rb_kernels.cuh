@@ -135,7 +135,16 @@ struct GemvStreamArgs {
   int* status;           // set to 2 when a pipeline wait gives up
   long long kslots;      // partial-state slots per output of a unit cut between CTAs
   int groups;            // thread groups per output (power of two, 1..8)
+  // failure-path test hook (rb_debug_pipeline_fault): each CTA's producer issues at most
+  // `stop_after` stages (< 0: all), and consumers give up waiting for a stage's data after
+  // `wait_polls` polls (0: the default ~2 s)
+  long long stop_after;
+  long long wait_polls;
 };
+
+// Failure-path test hook (rb_runtime.cu): stop_after / wait_polls for the next TMA-fed
+// kernels (stop_after < 0 and wait_polls 0 when unset).
+void pipeline_fault(long long* stop_after, long long* wait_polls);
 
 struct Blas23FoldOps {
   cudaError_t (*gemv)(const GemvArgs& g, bool rows, dim3 grid, cudaStream_t s);

@@ -37,9 +37,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t addr, unsigned parity) {
   return ok != 0;
 }
 
-// Bounded wait: gives up after ~2 s and reports false.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t addr, unsigned parity) {
-  for (long long it = 0; it < (1ll << 25); it++) {
+// Polls of a bounded wait: ~2 s. Waits for copies or tensor-core work already issued (the
+// drains before a CTA exits or frees TMEM) always use this limit.
+constexpr long long kWaitPolls = 1ll << 25;
+
+// Bounded wait: gives up after `polls` polls (default ~2 s) and reports false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t addr, unsigned parity,
+                                                  long long polls = kWaitPolls) {
+  for (long long it = 0; it < polls; it++) {
     if (mbar_try_wait(addr, parity)) return true;
     if (it > 1024) __nanosleep(64);
   }

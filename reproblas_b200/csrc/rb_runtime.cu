@@ -71,7 +71,57 @@ Mem classify(const void* p) {
   }
 }
 
+// ---- failure-path test hooks -----------------------------------------------------------------
+static std::atomic<int> g_fail_allocs{0};
+static std::atomic<long long> g_fault_stop_after{-1};
+static std::atomic<long long> g_fault_wait_polls{0};
+
+void pipeline_fault(long long* stop_after, long long* wait_polls) {
+  *stop_after = g_fault_stop_after.load();
+  *wait_polls = g_fault_wait_polls.load();
+}
+
+// cudaMalloc / cudaMallocHost, except that while the allocation-failure hook still has
+// failures to hand out, the next request fails as an exhausted device would.
+static bool hooked_failure() {
+  int n = g_fail_allocs.load();
+  while (n > 0)
+    if (g_fail_allocs.compare_exchange_weak(n, n - 1)) return true;
+  return false;
+}
+cudaError_t dev_malloc(void** p, size_t bytes) {
+  if (hooked_failure()) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(p, bytes);
+}
+static cudaError_t host_malloc(void** p, size_t bytes) {
+  if (hooked_failure()) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMallocHost(p, bytes);
+}
+
 // ---- workspace ------------------------------------------------------------------------------
+void Workspace::release() {
+  for (int i = 0; i < kRing; i++) {
+    for (int j = 0; j < 2; j++)
+      if (ring[i][j]) { cudaFree(ring[i][j]); ring[i][j] = nullptr; }
+    if (copied[i]) { cudaEventDestroy(copied[i]); copied[i] = nullptr; }
+    if (consumed[i]) { cudaEventDestroy(consumed[i]); consumed[i] = nullptr; }
+  }
+  ring_ready = false;
+  if (scratch.records) { cudaFree(scratch.records); scratch.records = nullptr; }
+  if (scratch.ticket) { cudaFree(scratch.ticket); scratch.ticket = nullptr; }
+  if (dsmall) { cudaFree(dsmall); dsmall = nullptr; }
+  if (hsmall) { cudaFreeHost(hsmall); hsmall = nullptr; }
+  if (big) { cudaFree(big); big = nullptr; big_bytes = 0; }
+  if (tickets) { cudaFree(tickets); tickets = nullptr; ntickets = 0; }
+  if (copy_stream) { cudaStreamDestroy(copy_stream); copy_stream = nullptr; }
+}
+
 bool Workspace::ensure_ring(size_t chunk) {
   if (ring_ready && chunk <= chunk_bytes) return true;
   for (int i = 0; i < kRing; i++)
@@ -79,7 +129,8 @@ bool Workspace::ensure_ring(size_t chunk) {
       if (ring[i][j]) { cudaFree(ring[i][j]); ring[i][j] = nullptr; }
   for (int i = 0; i < kRing; i++) {
     for (int j = 0; j < 2; j++)
-      if (cudaMalloc(&ring[i][j], chunk) != cudaSuccess) {
+      if (dev_malloc((void**)&ring[i][j], chunk) != cudaSuccess) {
+        ring[i][j] = nullptr;
         set_error(RB_ERR_ALLOC, "staging buffer allocation failed");
         return false;
       }
@@ -96,7 +147,8 @@ bool Workspace::ensure_big(size_t bytes) {
   // drain the stream first: kernels in flight may still read the old buffer
   if (!cuda_ok(cudaStreamSynchronize(stream), "cudaStreamSynchronize")) return false;
   if (big) { cudaFree(big); big = nullptr; big_bytes = 0; }
-  if (cudaMalloc(&big, bytes) != cudaSuccess) {
+  if (dev_malloc((void**)&big, bytes) != cudaSuccess) {
+    big = nullptr;
     set_error(RB_ERR_ALLOC, "workspace allocation failed");
     return false;
   }
@@ -110,7 +162,8 @@ bool Workspace::ensure_tickets(size_t n) {
   if (!cuda_ok(cudaStreamSynchronize(stream), "cudaStreamSynchronize")) return false;
   if (tickets) { cudaFree(tickets); tickets = nullptr; ntickets = 0; }
   size_t want = n < 65536 ? 65536 : n;
-  if (cudaMalloc(&tickets, want * sizeof(unsigned)) != cudaSuccess) {
+  if (dev_malloc((void**)&tickets, want * sizeof(unsigned)) != cudaSuccess) {
+    tickets = nullptr;
     set_error(RB_ERR_ALLOC, "ticket allocation failed");
     return false;
   }
@@ -138,16 +191,20 @@ static bool init_workspace(Workspace* w, int dev, cudaStream_t s, int sms) {
   // records for up to 16 CTAs per SM of the largest record (complex, fold 8)
   size_t rec = blas1_record_bytes(8, kMaxFold, 2);
   w->records_bytes = (size_t)sms * 16 * rec;
-  if (cudaMalloc(&w->scratch.records, w->records_bytes) != cudaSuccess ||
-      cudaMalloc(&w->scratch.ticket, 256) != cudaSuccess ||
-      cudaMalloc(&w->dsmall, Workspace::kSmallBytes) != cudaSuccess) {
+  if (dev_malloc(&w->scratch.records, w->records_bytes) != cudaSuccess ||
+      dev_malloc((void**)&w->scratch.ticket, 256) != cudaSuccess ||
+      dev_malloc((void**)&w->dsmall, Workspace::kSmallBytes) != cudaSuccess) {
     set_error(RB_ERR_ALLOC, "workspace allocation failed");
     return false;
   }
   if (!cuda_ok(cudaMemset(w->scratch.ticket, 0, 256), "cudaMemset") ||
       !cuda_ok(cudaMemset(w->dsmall, 0, Workspace::kSmallBytes), "cudaMemset"))
     return false;
-  if (!cuda_ok(cudaMallocHost(&w->hsmall, Workspace::kSmallBytes), "cudaMallocHost")) return false;
+  if (host_malloc((void**)&w->hsmall, Workspace::kSmallBytes) != cudaSuccess) {
+    w->hsmall = nullptr;
+    set_error(RB_ERR_ALLOC, "pinned workspace allocation failed");
+    return false;
+  }
   // the device's address of the pinned slots (kernels store value results straight there)
   if (!cuda_ok(cudaHostGetDevicePointer((void**)&w->hsmall_dev, w->hsmall, 0), "cudaHostGetDevicePointer"))
     return false;
@@ -157,7 +214,7 @@ static bool init_workspace(Workspace* w, int dev, cudaStream_t s, int sms) {
   return true;
 }
 
-Workspace* acquire_workspace(std::unique_lock<std::mutex>* lock) {
+Workspace* acquire_workspace(std::unique_lock<std::mutex>* lock, bool create) {
   static std::mutex mu;
   static std::map<std::pair<int, cudaStream_t>, std::unique_ptr<Workspace>> table;
   DeviceInfo di;
@@ -169,8 +226,12 @@ Workspace* acquire_workspace(std::unique_lock<std::mutex>* lock) {
     auto key = std::make_pair(di.device, s);
     auto it = table.find(key);
     if (it == table.end()) {
+      if (!create) return nullptr;
       std::unique_ptr<Workspace> nw(new Workspace());
-      if (!init_workspace(nw.get(), di.device, s, di.sms)) return nullptr;
+      if (!init_workspace(nw.get(), di.device, s, di.sms)) {
+        nw->release();   // a later call on this stream starts over
+        return nullptr;
+      }
       it = table.emplace(key, std::move(nw)).first;
     }
     w = it->second.get();
@@ -217,6 +278,35 @@ void rb_set_launch_config(int ctas_per_sm, int threads_per_cta) {
   rb::g_threads.store(threads_per_cta);
 }
 unsigned long long rb_kernel_launch_count(void) { return rb::g_launches.load(); }
+
+int rb_synchronize(void) {
+  cudaStream_t s = rb::current_stream();
+  if (!rb::cuda_ok(cudaStreamSynchronize(s), "rb_synchronize: cudaStreamSynchronize"))
+    return RB_ERR_CUDA;
+  std::unique_lock<std::mutex> lock;
+  rb::Workspace* w = rb::acquire_workspace(&lock, false);
+  if (!w) return RB_SUCCESS;   // no call has run on this stream
+  int* hs = w->hstatus();
+  if (!rb::cuda_ok(cudaMemcpyAsync(hs, w->dstatus(), 4, cudaMemcpyDeviceToHost, s), "copy status") ||
+      !rb::cuda_ok(cudaStreamSynchronize(s), "cudaStreamSynchronize"))
+    return RB_ERR_CUDA;
+  if (*hs != 0) {
+    if (!rb::cuda_ok(cudaMemsetAsync(w->dstatus(), 0, 4, s), "cudaMemsetAsync") ||
+        !rb::cuda_ok(cudaStreamSynchronize(s), "cudaStreamSynchronize"))
+      return RB_ERR_CUDA;
+    rb::set_error(RB_ERR_CUDA, "a pipeline wait timed out in an earlier call on this stream "
+                               "(its affected outputs are NaN)");
+    return RB_ERR_CUDA;
+  }
+  return RB_SUCCESS;
+}
+
+void rb_debug_fail_allocations(int count) { rb::g_fail_allocs.store(count > 0 ? count : 0); }
+
+void rb_debug_pipeline_fault(long long stop_after, long long wait_polls) {
+  rb::g_fault_stop_after.store(stop_after);
+  rb::g_fault_wait_polls.store(wait_polls > 0 ? wait_polls : 0);
+}
 const char* rb_version(void) { return "reproblas_b200 0.1 (sm_100a)"; }
 
 }  // extern "C"
