@@ -24,12 +24,18 @@
  * synchronise that stream before returning. binnedBLAS_* calls whose accumulator and
  * inputs are all in device memory only enqueue work.
  *
- * Errors: the reference has no error returns. Here invalid arguments (fold outside 2..8,
+ * Errors: the reference has no error returns. Here invalid arguments (fold outside 2..52,
  * negative strides, misaligned element pointers) and CUDA failures set a thread-local error
  * (rb_get_last_error); value-returning functions then return NaN and others leave their
  * outputs untouched. N <= 0 behaves as in the reference (nothing is deposited).
  *
- * Supported folds: 2..8 (the reference default is 3, DIDEFAULTFOLD / SIDEFAULTFOLD).
+ * Supported folds: every fold the reference accepts, 2 up to binned_DBMAXFOLD = 52 for FP64
+ * and double complex elements and binned_SBMAXFOLD = 21 for FP32 and float complex elements
+ * (include/binned.h:123,131); the reference default is 3 (DIDEFAULTFOLD / SIDEFAULTFOLD).
+ * Folds 2..8 run register-resident kernels; larger folds a run-time fold path (state in
+ * local memory, one thread per gemv / gemm entry) with the same bits. Exceptions, each
+ * documented at its declaration: rb_dgemm_int8 and the batched plans take folds 2..4,
+ * rb_ddot_noalloc folds 2..8.
  */
 #ifndef REPROBLAS_B200_H
 #define REPROBLAS_B200_H
@@ -481,7 +487,7 @@ void rb_batch_plan_destroy(rb_batch_plan *plan);
 /* Error codes of the thread-local error side channel. */
 enum {
   RB_SUCCESS = 0,
-  RB_ERR_INVALID_ARG = 1,    /* fold outside 2..8, negative stride, bad Order/Trans, ... */
+  RB_ERR_INVALID_ARG = 1,    /* fold outside 2..52 (2..21), negative stride, bad Order/Trans */
   RB_ERR_CUDA = 2,           /* a CUDA runtime call failed (message has the details) */
   RB_ERR_ALLOC = 3,          /* device or pinned allocation failed */
   RB_ERR_UNSUPPORTED = 4     /* a valid request this build does not implement */

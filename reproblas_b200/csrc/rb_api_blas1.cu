@@ -1,7 +1,8 @@
 // rb_api_blas1.cu -- C ABI for the BLAS1 reductions (reproBLAS_* / binnedBLAS_* names).
 //
 // Every entry point funnels into run_blas1(), which
-//   * validates the arguments the way the reference would accept them (fold 2..8 here),
+//   * validates the arguments the way the reference would accept them (fold 2 up to
+//     binned_DBMAXFOLD = 52 for FP64 elements, binned_SBMAXFOLD = 21 for FP32 elements),
 //   * places the binned accumulator on the device (the caller's device accumulator is
 //     used in place; a host accumulator is copied in and back; value-returning calls use
 //     a zeroed workspace slot, as the reference's reproBLAS_r* wrappers zero theirs),
@@ -77,8 +78,9 @@ void plan_vector(const Blas1Req& r, const void* x, long long incx, const void* y
 }
 
 bool run_blas1(const Blas1Req& r) {
-  if (r.fold < 2 || r.fold > kMaxFold) {
-    set_error(RB_ERR_INVALID_ARG, "fold must be in [2, 8]");
+  if (r.fold < 2 || r.fold > max_fold(r.type)) {
+    set_error(RB_ERR_INVALID_ARG, max_fold(r.type) == kMaxFoldD ? "fold must be in [2, 52]"
+                                                                 : "fold must be in [2, 21]");
     return false;
   }
   if (r.incx < 0 || (is_dot(r) && r.incy < 0)) {
@@ -141,6 +143,7 @@ bool run_blas1(const Blas1Req& r) {
 
   Blas1Args a{};
   a.scratch = w->scratch;
+  a.fold = r.fold;
   a.acc = dacc;
   a.scale = ssq ? w->dscale() : nullptr;
   a.sqrt_result = r.sqrt_result ? 1 : 0;
@@ -271,8 +274,8 @@ bool complex_asum(char rt, int fold, int N, const void* X, int incX, void* acc, 
     set_error(RB_ERR_INVALID_ARG, "negative or too large stride");
     return false;
   }
-  double tmp[2 * kMaxFold] = {};   // host state when the caller gave none (reals are 8 bytes)
-  float tmpf[2 * kMaxFold] = {};
+  double tmp[2 * kMaxFoldD] = {};   // host state when the caller gave none (reals are 8 bytes)
+  float tmpf[2 * kMaxFoldS] = {};
   void* st = acc ? acc : (rt == 'd' ? (void*)tmp : (void*)tmpf);
   Blas1Req re{rt, kOpAsum, fold, N, X, 2 * incX, nullptr, 0, st, 0.0, nullptr, nullptr, false};
   Blas1Req im{rt, kOpAsum, fold, N, (const unsigned char*)X + cb, 2 * incX, nullptr, 0, st, 0.0,
@@ -296,8 +299,8 @@ bool complex_ssq(char rt, int fold, int N, const void* X, int incX, void* acc, d
     set_error(RB_ERR_INVALID_ARG, "negative or too large stride");
     return false;
   }
-  double tmp[2 * kMaxFold] = {};
-  float tmpf[2 * kMaxFold] = {};
+  double tmp[2 * kMaxFoldD] = {};
+  float tmpf[2 * kMaxFoldS] = {};
   void* st = acc ? acc : (rt == 'd' ? (void*)tmp : (void*)tmpf);
   double s1 = 0.0;
   Blas1Req re{rt, kOpSsq, fold, N, X, 2 * incX, nullptr, 0, st, scale_in, &s1, nullptr, false};
@@ -552,8 +555,8 @@ void binnedBLAS_cbcsum(const int fold, const int N, const void* X, const int inc
 // ---- state merge (no reference counterpart as one call) --------------------------------------
 int rb_dbdbadd_states(const int fold, const int count, const double_binned* states,
                       double_binned* out) {
-  if (fold < 2 || fold > rb::kMaxFold || count < 0) {
-    rb::set_error(RB_ERR_INVALID_ARG, "rb_dbdbadd_states: fold must be in [2, 8], count >= 0");
+  if (fold < 2 || fold > rb::kMaxFoldD || count < 0) {
+    rb::set_error(RB_ERR_INVALID_ARG, "rb_dbdbadd_states: fold must be in [2, 52], count >= 0");
     return RB_ERR_INVALID_ARG;
   }
   if (count > 0 && (!rb::on_device(states) || !rb::on_device(out))) {

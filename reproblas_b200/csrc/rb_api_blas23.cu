@@ -218,8 +218,11 @@ bool run_gemv_stream(const GemvReq& q, const Blas23FoldOps* o, Workspace* w, con
 
 bool run_gemv(const GemvReq& q) {
   if (q.M == 0 || q.N == 0) return true;   // rdgemv.c:43-45
-  const Blas23FoldOps* o = ops23(q.fold);
-  if (!o) { set_error(RB_ERR_INVALID_ARG, "fold must be in [2, 8]"); return false; }
+  if (q.fold < 2 || q.fold > kMaxFoldD) {
+    set_error(RB_ERR_INVALID_ARG, "fold must be in [2, 52]");
+    return false;
+  }
+  const Blas23FoldOps* o = q.fold <= kMaxFold ? ops23(q.fold) : nullptr;
   if (q.M < 0 || q.N < 0 || q.lda < 1 || q.incX < 0 || q.incY < 1) {
     set_error(RB_ERR_INVALID_ARG, "gemv: negative size, lda < 1, incX < 0 or incY < 1");
     return false;
@@ -232,6 +235,19 @@ bool run_gemv(const GemvReq& q) {
   const long long nout = nt ? Rs : Cs, nred = nt ? Cs : Rs;
   const long long nred_eff = q.alpha == 0.0 ? 0 : nred;   // dbdgemv.ccog:70-72
   if (q.mode == kOutBinned && nred_eff == 0) return true;  // binnedBLAS_dbdgemv touches nothing
+  if (!o) {
+    // folds above the register-resident kernels: one thread per entry (rb_foldn.cu)
+    EntryReq<double> e{};
+    e.fold = q.fold;
+    e.mode = q.mode;
+    e.M = nout; e.N = 1; e.K = nred_eff;
+    e.A = q.A; e.sai = nt ? q.lda : 1; e.sak = nt ? 1 : q.lda;
+    e.B = q.X; e.sbk = q.incX; e.sbj = 0;
+    e.ar = q.alpha; e.br = q.beta;
+    e.alpha_on_b = true;
+    e.C = q.Y; e.sci = q.incY; e.scj = 0;
+    return run_entries_n<double, false>(e);
+  }
 
   std::unique_lock<std::mutex> lock;
   Workspace* w = acquire_workspace(&lock);
@@ -366,8 +382,11 @@ struct GemmReq {
 
 bool run_gemm(const GemmReq& q) {
   if (q.M == 0 || q.N == 0) return true;   // rdgemm.c:50-52
-  const Blas23FoldOps* o = ops23(q.fold);
-  if (!o) { set_error(RB_ERR_INVALID_ARG, "fold must be in [2, 8]"); return false; }
+  if (q.fold < 2 || q.fold > kMaxFoldD) {
+    set_error(RB_ERR_INVALID_ARG, "fold must be in [2, 52]");
+    return false;
+  }
+  const Blas23FoldOps* o = q.fold <= kMaxFold ? ops23(q.fold) : nullptr;
   if (q.M < 0 || q.N < 0 || q.K < 0 || q.lda < 1 || q.ldb < 1 || q.ldc < 1) {
     set_error(RB_ERR_INVALID_ARG, "gemm: negative size or leading dimension < 1");
     return false;
@@ -390,6 +409,18 @@ bool run_gemm(const GemmReq& q) {
   g.beta = q.beta;
   g.mode = q.mode;
   if (q.mode == kOutBinned && g.K == 0) return true;   // binnedBLAS_dbdgemm touches nothing
+  if (!o) {
+    // folds above the register-resident kernels: one thread per entry (rb_foldn.cu)
+    EntryReq<double> e{};
+    e.fold = q.fold;
+    e.mode = q.mode;
+    e.M = g.M; e.N = g.N; e.K = g.K;
+    e.A = q.A; e.sai = g.sai; e.sak = g.sak;
+    e.B = q.B; e.sbk = g.sbk; e.sbj = g.sbj;
+    e.ar = q.alpha; e.br = q.beta;
+    e.C = q.C; e.sci = g.sci; e.scj = g.scj;
+    return run_entries_n<double, false>(e);
+  }
 
   std::unique_lock<std::mutex> lock;
   Workspace* w = acquire_workspace(&lock);

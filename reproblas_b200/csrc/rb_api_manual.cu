@@ -26,7 +26,7 @@ struct Manual {
   int incpri;
   T* car;
   int inccar;
-  T st[4 * kMaxFold];
+  T st[4 * kMaxFoldD];
 
   // Copy `fold` rows of `comps` elements between a strided array and a contiguous one.
   static bool move(T* dst, size_t dpitch, const T* src, size_t spitch, size_t width, int rows,
@@ -37,8 +37,10 @@ struct Manual {
   }
 
   bool valid(const char* name) const {
-    if (fold < 2 || fold > kMaxFold) {
-      set_error(RB_ERR_INVALID_ARG, std::string(name) + ": fold must be in [2, 8]");
+    const int maxf = sizeof(T) == 8 ? kMaxFoldD : kMaxFoldS;
+    if (fold < 2 || fold > maxf) {
+      set_error(RB_ERR_INVALID_ARG, std::string(name) + ": fold must be in [2, " +
+                                        std::to_string(maxf) + "]");
       return false;
     }
     if (!pri || !car || incpri < 1 || inccar < 1) {

@@ -16,6 +16,7 @@
 // over the M rows (zbzgemv.ccog:214-218, cbcgemv.ccog:214-218), which equals the mathematical
 // A^H x only when M == N. Here every entry is the full A^H x.
 #include <cstring>
+#include <string>
 
 #include "rb_host.h"
 #include "../../include/reproblas_b200.h"
@@ -27,6 +28,7 @@ bool xrow(char o) { return o == 'r' || o == 'R'; }
 bool xnt(char t) { return t == 'n' || t == 'N'; }
 bool xplain_t(char t) { return t == 't' || t == 'T'; }
 
+// The fixed-fold kernels (folds 2..8); nullptr above them, where the run-time fold path runs.
 template <typename E, bool CX>
 const XOps<E>* xops_for(int fold) {
   if (fold < 2 || fold > kMaxFold) return nullptr;
@@ -68,8 +70,12 @@ template <typename E, bool CX>
 bool run_xgemv(const XGemvReq<E, CX>& q) {
   constexpr int NC = CX ? 2 : 1;
   if (q.M == 0 || q.N == 0) return true;   // r[szc]gemv.c: early return
+  const int maxf = sizeof(E) == 8 ? kMaxFoldD : kMaxFoldS;
+  if (q.fold < 2 || q.fold > maxf) {
+    set_error(RB_ERR_INVALID_ARG, "fold must be in [2, " + std::to_string(maxf) + "]");
+    return false;
+  }
   const XOps<E>* o = xops_for<E, CX>(q.fold);
-  if (!o) { set_error(RB_ERR_INVALID_ARG, "fold must be in [2, 8]"); return false; }
   if (q.M < 0 || q.N < 0 || q.lda < 1 || q.incX < 0 || q.incY < 1) {
     set_error(RB_ERR_INVALID_ARG, "gemv: negative size, lda < 1, incX < 0 or incY < 1");
     return false;
@@ -84,6 +90,20 @@ bool run_xgemv(const XGemvReq<E, CX>& q) {
   const bool alpha_zero = q.alpha.r == E(0) && q.alpha.i == E(0);
   const long long nred_eff = alpha_zero ? 0 : nred;            // [szc]b[szc]gemv: alpha == 0
   if (q.mode == kOutBinned && nred_eff == 0) return true;       // binned form touches nothing
+  if (!o) {
+    // folds above the register-resident kernels: one thread per entry (rb_foldn.cu)
+    EntryReq<E> e{};
+    e.fold = q.fold;
+    e.mode = q.mode;
+    e.M = nout; e.N = 1; e.K = nred_eff;
+    e.A = q.A; e.sai = nt ? q.lda : 1; e.sak = nt ? 1 : q.lda;
+    e.B = q.X; e.sbk = q.incX; e.sbj = 0;
+    e.ar = q.alpha.r; e.ai = q.alpha.i; e.br = q.beta.r; e.bi = q.beta.i;
+    e.alpha_on_b = true;
+    e.conja = conj;
+    e.C = q.Y; e.sci = q.incY; e.scj = 0;
+    return run_entries_n<E, CX>(e);
+  }
 
   std::unique_lock<std::mutex> lock;
   Workspace* w = acquire_workspace(&lock);
@@ -239,8 +259,12 @@ template <typename E, bool CX>
 bool run_xgemm(const XGemmReq<E, CX>& q) {
   constexpr int NC = CX ? 2 : 1;
   if (q.M == 0 || q.N == 0) return true;   // r[szc]gemm.c: early return
+  const int maxf = sizeof(E) == 8 ? kMaxFoldD : kMaxFoldS;
+  if (q.fold < 2 || q.fold > maxf) {
+    set_error(RB_ERR_INVALID_ARG, "fold must be in [2, " + std::to_string(maxf) + "]");
+    return false;
+  }
   const XOps<E>* o = xops_for<E, CX>(q.fold);
-  if (!o) { set_error(RB_ERR_INVALID_ARG, "fold must be in [2, 8]"); return false; }
   if (q.M < 0 || q.N < 0 || q.K < 0 || q.lda < 1 || q.ldb < 1 || q.ldc < 1) {
     set_error(RB_ERR_INVALID_ARG, "gemm: negative size or leading dimension < 1");
     return false;
@@ -269,6 +293,20 @@ bool run_xgemm(const XGemmReq<E, CX>& q) {
   g.conjb = (CX && tb && !xplain_t(q.tb)) ? 1 : 0;
   g.mode = q.mode;
   if (q.mode == kOutBinned && g.K == 0) return true;   // binned form touches nothing
+  if (!o) {
+    // folds above the register-resident kernels: one thread per entry (rb_foldn.cu)
+    EntryReq<E> e{};
+    e.fold = q.fold;
+    e.mode = q.mode;
+    e.M = g.M; e.N = g.N; e.K = g.K;
+    e.A = q.A; e.sai = g.sai; e.sak = g.sak;
+    e.B = q.B; e.sbk = g.sbk; e.sbj = g.sbj;
+    e.ar = g.ar; e.ai = g.ai; e.br = g.br; e.bi = g.bi;
+    e.conja = g.conja != 0;
+    e.conjb = g.conjb != 0;
+    e.C = q.C; e.sci = g.sci; e.scj = g.scj;
+    return run_entries_n<E, CX>(e);
+  }
 
   std::unique_lock<std::mutex> lock;
   Workspace* w = acquire_workspace(&lock);

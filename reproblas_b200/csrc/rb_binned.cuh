@@ -454,9 +454,9 @@ __device__ __forceinline__ void tileN(Acc<T, F> (&a)[N], const T (&v)[N][K]) {
 }
 
 // binned_ddmconv (src/binned/ddmconv.c:23-81): fixed-order conversion to double with
-// scaling when the index is within 3 of the top.
-template <int F>
-__device__ inline double conv(const double* pri, const double* car, int inc) {
+// scaling when the index is within 3 of the top. `F` is the fold (any fold; the template
+// form below serves the kernels of a fixed fold).
+__device__ inline double conv_n(const int F, const double* pri, const double* car, int inc) {
   using B = BT<double>;
   double p0 = pri[0];
   if ((B::bits(p0) & B::kAbsMask) >= 0x7ff0000000000000ull) return p0;
@@ -504,9 +504,13 @@ __device__ inline double conv(const double* pri, const double* car, int inc) {
   return Y;
 }
 
-// binned_ssmconv (src/binned/ssmconv.c:22-57): accumulated in double, rounded to float.
 template <int F>
-__device__ inline float sconv(const float* pri, const float* car, int inc) {
+__device__ __forceinline__ double conv(const double* pri, const double* car, int inc) {
+  return conv_n(F, pri, car, inc);
+}
+
+// binned_ssmconv (src/binned/ssmconv.c:22-57): accumulated in double, rounded to float.
+__device__ inline float sconv_n(const int F, const float* pri, const float* car, int inc) {
   using B = BT<float>;
   float p0 = pri[0];
   if ((B::bits(p0) & B::kAbsMask) >= 0x7f800000u) return p0;
@@ -529,6 +533,11 @@ __device__ inline float sconv(const float* pri, const float* car, int inc) {
   }
   Y = __dadd_rn(Y, (double)__fsub_rn(pri[(F - 1) * inc], B::bin(X_index + F - 1)));
   return __double2float_rn(Y);
+}
+
+template <int F>
+__device__ __forceinline__ float sconv(const float* pri, const float* car, int inc) {
+  return sconv_n(F, pri, car, inc);
 }
 
 }  // namespace rb

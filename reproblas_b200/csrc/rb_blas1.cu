@@ -9,9 +9,12 @@
 
 namespace rb {
 
-bool fold_supported(int fold) { return fold >= 2 && fold <= kMaxFold; }
+bool fold_supported(int fold) { return fold >= 2 && fold <= kMaxFoldD; }
 
+// The fixed-fold kernels for folds 2..8, the run-time fold kernels above (the caller checks
+// the fold against the element type's maximum).
 static const Blas1FoldOps* fold_ops(int fold) {
+  if (fold > kMaxFold && fold <= kMaxFoldD) return &blas1_fold_n;
   switch (fold) {
     case 2: return &blas1_fold2;
     case 3: return &blas1_fold3;
@@ -46,6 +49,7 @@ cudaError_t launch_blas1_c(int fold, int op, bool vec, int grid, int block, cons
 }
 cudaError_t launch_merge_states(int fold, int count, const double* states, double* out,
                                 cudaStream_t s) {
+  if (fold > kMaxFold) return merge_states_n('d', false, fold, count, states, out, s);
   const Blas1FoldOps* o = fold_ops(fold);
   return o ? o->merge(count, states, out, s) : cudaErrorInvalidValue;
 }

@@ -68,15 +68,17 @@ struct Workspace {
   unsigned* tickets = nullptr;
   size_t ntickets = 0;
 
-  double* dacc() { return (double*)dsmall; }                  // 1024 B accumulator slot
-  int* dstatus() { return (int*)(dsmall + 2048); }             // kernel status word (0 = ok)
-  int* hstatus() { return (int*)(hsmall + 2048); }
-  double* dscale() { return (double*)(dsmall + 1024); }        // 8 B
-  void* dresult() { return (void*)(dsmall + 1088); }           // 64 B result slot
+  // dsmall layout: [0, 2048) accumulator (a complex FP64 state of fold 52 is 1664 bytes),
+  // 2048 scale, 2112 result (64 bytes), 2304 kernel status word
+  double* dacc() { return (double*)dsmall; }
+  int* dstatus() { return (int*)(dsmall + 2304); }             // kernel status word (0 = ok)
+  int* hstatus() { return (int*)(hsmall + 2304); }
+  double* dscale() { return (double*)(dsmall + 2048); }        // 8 B
+  void* dresult() { return (void*)(dsmall + 2112); }           // 64 B result slot
   double* hacc() { return (double*)hsmall; }
-  double* hscale() { return (double*)(hsmall + 1024); }
-  void* hresult() { return (void*)(hsmall + 1088); }
-  void* hresult_dev() { return (void*)(hsmall_dev + 1088); }   // hresult() as kernels address it
+  double* hscale() { return (double*)(hsmall + 2048); }
+  void* hresult() { return (void*)(hsmall + 2112); }
+  void* hresult_dev() { return (void*)(hsmall_dev + 2112); }   // hresult() as kernels address it
 
   bool ensure_ring(size_t chunk);
   bool ensure_big(size_t bytes);
@@ -97,6 +99,28 @@ int reduction_grid(long long work, int elems_per_thread, int threads, int occupa
 
 // Occupancy of the reduction kernels (CTAs per SM) for the chosen launch shape.
 int blas1_occupancy(char type, int fold, int op, bool vec, int threads);
+
+// ---- gemv / gemm entries at a run-time fold (rb_foldn.cu) ---------------------------------
+// C_ij <- conv( binned(beta*C_ij) + sum_k a_ik b_kj ) (kOutValue), or the binned state of C_ij
+// (kOutBinned) += sum_k a_ik b_kj, for i < M, j < N, with op(A)_ik = A[i*sai + k*sak],
+// op(B)_kj = B[k*sbk + j*sbj] (conjugated when conja / conjb), alpha multiplying op(B)
+// (alpha_on_b: gemv's x) or op(A), entry (i, j) at C + (i*sci + j*scj) values or states.
+// Host or device operands. E is the real element type; complex elements are pairs.
+template <typename E>
+struct EntryReq {
+  int fold, mode;
+  long long M, N, K;
+  const void* A;
+  long long sai, sak;
+  const void* B;
+  long long sbk, sbj;
+  E ar, ai, br, bi;
+  bool alpha_on_b, conja, conjb;
+  void* C;
+  long long sci, scj;
+};
+template <typename E, bool CX>
+bool run_entries_n(const EntryReq<E>& q);
 
 // ---- operand staging for the BLAS2/3 entry points ------------------------------------------
 // Bump allocator over the workspace's big buffer (one call at a time holds the workspace).

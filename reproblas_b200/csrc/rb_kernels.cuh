@@ -26,6 +26,7 @@ enum OpC : int {
 struct GridScratch {
   void* records;       // >= gridDim.x * record_bytes
   unsigned* ticket;    // zero on entry, zero again on exit
+  size_t bytes;        // capacity of `records`
 };
 
 struct Blas1Args {
@@ -41,6 +42,7 @@ struct Blas1Args {
   double* scale;             // ssq: device scale, read then written (may be null: 0)
   void* result;              // device converted result (T, or 2 T for complex); may be null
   int sqrt_result;           // ssq: write scale*sqrt(conv) instead of conv
+  int fold;                  // the fold (read by the run-time fold kernels)
 };
 
 // Launch helpers implemented in rb_blas1.cu; return cudaSuccess or the launch error.
@@ -213,6 +215,19 @@ extern const XOps<double> xops_z[7];   // rb_xblas23_z.cu
 extern const XOps<float> xops_c[7];    // rb_xblas23_c.cu
 
 bool fold_supported(int fold);
+// Folds of the register-resident kernels (2..kMaxFold, a template parameter) and the largest
+// folds the reference accepts, binned_DBMAXFOLD and binned_SBMAXFOLD (include/binned.h:123,
+// 131), served above kMaxFold by the run-time fold kernels of rb_foldn.cu.
 constexpr int kMaxFold = 8;
+constexpr int kMaxFoldD = 52;
+constexpr int kMaxFoldS = 21;
+// largest fold for elements of real type 'd' / 'z' (FP64) or 's' / 'c' (FP32)
+inline int max_fold(char type) { return (type == 'd' || type == 'z') ? kMaxFoldD : kMaxFoldS; }
+
+// ---- run-time fold kernels (rb_foldn.cu) -------------------------------------------------
+extern const Blas1FoldOps blas1_fold_n;   // reads the fold from Blas1Args::fold
+// merge `count` packed states of kind 'd', 's', 'z', 'c' (sq: [scale, state] records)
+cudaError_t merge_states_n(char kind, bool sq, int fold, int count, const void* states,
+                           void* out, cudaStream_t s);
 
 }  // namespace rb

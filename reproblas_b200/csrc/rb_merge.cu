@@ -111,8 +111,10 @@ cudaError_t launch_kind(int fold, int count, const void* states, void* out, cuda
 // Validation shared by the entry points; returns an RB_* code.
 template <typename T, bool CX, bool SQ>
 int merge_entry(const char* name, int fold, int count, const void* states, void* out) {
-  if (fold < 2 || fold > kMaxFold || count < 0) {
-    set_error(RB_ERR_INVALID_ARG, std::string(name) + ": fold must be in [2, 8], count >= 0");
+  const int maxf = sizeof(T) == 8 ? kMaxFoldD : kMaxFoldS;
+  if (fold < 2 || fold > maxf || count < 0) {
+    set_error(RB_ERR_INVALID_ARG, std::string(name) + ": fold must be in [2, " +
+                                      std::to_string(maxf) + "], count >= 0");
     return RB_ERR_INVALID_ARG;
   }
   if (count > 0 && (!on_device(states) || !on_device(out))) {
@@ -121,8 +123,11 @@ int merge_entry(const char* name, int fold, int count, const void* states, void*
   }
   if (count == 0) return RB_SUCCESS;
   count_launch();
-  if (!cuda_ok(launch_kind<T, CX, SQ>(fold, count, states, out, current_stream()), "kernel launch"))
-    return RB_ERR_CUDA;
+  const char kind = CX ? (sizeof(T) == 8 ? 'z' : 'c') : (sizeof(T) == 8 ? 'd' : 's');
+  const cudaError_t e = fold > kMaxFold
+                            ? merge_states_n(kind, SQ, fold, count, states, out, current_stream())
+                            : launch_kind<T, CX, SQ>(fold, count, states, out, current_stream());
+  if (!cuda_ok(e, "kernel launch")) return RB_ERR_CUDA;
   return RB_SUCCESS;
 }
 

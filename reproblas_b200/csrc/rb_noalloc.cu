@@ -89,7 +89,8 @@ extern "C" int rb_ddot_noalloc(const int fold, const int N, const double* X, con
                                double* result, void* stream) {
   using namespace rb;
   if (fold < 2 || fold > kMaxFold) {
-    set_error(RB_ERR_INVALID_ARG, "rb_ddot_noalloc: fold must be in [2, 8]");
+    set_error(RB_ERR_INVALID_ARG, "rb_ddot_noalloc: fold must be in [2, 8] (the folds of the "
+                                  "register-resident kernels)");
     return RB_ERR_INVALID_ARG;
   }
   if (incX < 0 || incY < 0) {
@@ -157,6 +158,8 @@ extern "C" int rb_ddot_noalloc(const int fold, const int N, const double* X, con
   a.head = head; a.body_end = body_end;
   a.scratch.ticket = (unsigned*)base;
   a.scratch.records = base + kNoallocTicketBytes;
+  a.scratch.bytes = kNoallocScratchBytes - kNoallocTicketBytes;
+  a.fold = fold;
   a.acc = Z;
   a.scale = nullptr;
   a.result = result;

@@ -191,6 +191,7 @@ static bool init_workspace(Workspace* w, int dev, cudaStream_t s, int sms) {
   // records for up to 16 CTAs per SM of the largest record (complex, fold 8)
   size_t rec = blas1_record_bytes(8, kMaxFold, 2);
   w->records_bytes = (size_t)sms * 16 * rec;
+  w->scratch.bytes = w->records_bytes;
   if (dev_malloc(&w->scratch.records, w->records_bytes) != cudaSuccess ||
       dev_malloc((void**)&w->scratch.ticket, 256) != cudaSuccess ||
       dev_malloc((void**)&w->dsmall, Workspace::kSmallBytes) != cudaSuccess) {

@@ -29,7 +29,11 @@ def test_invalid_fold_sets_error(rb):
     assert rb.lib.rb_get_last_error() == 1
     assert b"fold" in rb.lib.rb_get_last_error_message()
     rb.lib.rb_clear_error()
-    v = rb.lib.reproBLAS_rdsum(9, 4, x.ctypes.data, 1)
+    # binned_DBMAXFOLD = 52 and binned_SBMAXFOLD = 21 are the largest folds
+    v = rb.lib.reproBLAS_rdsum(53, 4, x.ctypes.data, 1)
+    assert math.isnan(v) and rb.lib.rb_get_last_error() == 1
+    rb.lib.rb_clear_error()
+    v = rb.lib.reproBLAS_rssum(22, 4, x.astype(np.float32).ctypes.data, 1)
     assert math.isnan(v) and rb.lib.rb_get_last_error() == 1
     rb.lib.rb_clear_error()
 

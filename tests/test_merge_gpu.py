@@ -108,7 +108,7 @@ def test_scaled_state_merge(cuda, rb, port, kind, fold):
 def test_merge_errors(cuda, rb):
     s = dev(cuda, np.zeros(12, np.float32))
     with pytest.raises(rb.ReproBLASError):
-        rb.call("rb_cbcbadd_states", 9, 1, s, s)
+        rb.call("rb_cbcbadd_states", 22, 1, s, s)   # above binned_SBMAXFOLD
     with pytest.raises(rb.ReproBLASError):
         rb.call("rb_sbsbadd_states", 3, 1, np.zeros(6, np.float32), s)
     assert rb.call("rb_zbzbadd_states", 3, 0, None, None) == 0

@@ -570,3 +570,142 @@ def test_port_matches_reference_state_merges(port):
         s1 = port.sbsbaddsq(fold, sa, ptr(za), sb, ptr(p))
         s2 = R.sbsbaddsq(fold, sa, ptr(za), sb, ptr(q))
         assert same_value(np.float32(s1), np.float32(s2)) and same_state(p, q, fold), trial
+
+
+@pytest.mark.parametrize("fold", [9, 16, 52])
+def test_port_matches_reference_high_folds(port, fold):
+    """Folds above 8 up to binned_DBMAXFOLD (FP64 / double complex): the oracle equals the
+    compiled reference bit for bit (the GPU's run-time fold path is checked against it)."""
+    R = ref()
+    if R is None:
+        pytest.skip("reference library not built")
+    rng = np.random.default_rng(fold)
+    n = 5003
+    x = np.exp2(rng.uniform(-300, 300, n)) * rng.choice([-1.0, 1.0], n)
+    y = rng.standard_normal(n)
+    for name, args in (("dbdsum", (ptr(x), 1)), ("dbdasum", (ptr(x), 1)),
+                       ("dbddot", (ptr(x), 1, ptr(y), 1))):
+        a, b = binned_zeros(fold), binned_zeros(fold)
+        getattr(port, name)(fold, n, *args, ptr(a))
+        getattr(R, name)(fold, n, *args, ptr(b))
+        assert same_bits(a, b), (name, fold)
+    a, b = binned_zeros(fold), binned_zeros(fold)
+    assert port.dbdssq(fold, n, ptr(x), 1, 0.0, ptr(a)) == R.dbdssq(fold, n, ptr(x), 1, 0.0, ptr(b))
+    assert same_bits(a, b)
+    xz = (x + 1j * np.roll(y, 5)).astype(np.complex128)
+    yz = (y + 1j * np.roll(x, 7)).astype(np.complex128)
+    for name in ("zbzsum", "zbzdotc", "zbzdotu"):
+        a, b = binned_zeros(fold, "z"), binned_zeros(fold, "z")
+        args = (ptr(xz), 1) if name == "zbzsum" else (ptr(xz), 1, ptr(yz), 1)
+        getattr(port, name)(fold, n, *args, ptr(a))
+        getattr(R, name)(fold, n, *args, ptr(b))
+        assert same_bits(a, b), (name, fold)
+    a, b = binned_zeros(fold), binned_zeros(fold)
+    assert port.dbzssq(fold, n, ptr(xz), 1, 0.0, ptr(a)) == R.dbzssq(fold, n, ptr(xz), 1, 0.0, ptr(b))
+    assert same_bits(a, b)
+    assert same_value(port.rdnrm2(fold, n, ptr(x), 1), R.rdnrm2(fold, n, ptr(x), 1))
+    # merges and the 2-D routines
+    a, b = binned_zeros(fold), binned_zeros(fold)
+    port.dbdsum(fold, n, ptr(x), 1, ptr(a))
+    R.dbdsum(fold, n, ptr(y), 1, ptr(b))
+    c = b.copy()
+    port.dbdbadd(fold, ptr(a), ptr(b))
+    R.dbdbadd(fold, ptr(a), ptr(c))
+    assert same_bits(b, c)
+    M, N, K = 19, 23, 29
+    for order in "rc":
+        for ta in "nt":
+            A = rng.uniform(-1, 1, M * N)
+            lda = N if order == "r" else M
+            lx, ly = (N, M) if ta == "n" else (M, N)
+            xv, yv = rng.uniform(-1, 1, lx), rng.uniform(-1, 1, ly)
+            ya, yb = yv.copy(), yv.copy()
+            port.rdgemv(fold, order.encode(), ta.encode(), M, N, 1.5, ptr(A), lda, ptr(xv), 1, 0.5, ptr(ya), 1)
+            R.rdgemv(fold, order.encode(), ta.encode(), M, N, 1.5, ptr(A), lda, ptr(xv), 1, 0.5, ptr(yb), 1)
+            assert same_bits(ya, yb), ("rdgemv", order, ta)
+        A, B, C = rng.uniform(-1, 1, M * K), rng.uniform(-1, 1, K * N), rng.uniform(-1, 1, M * N)
+        lda, ldb, ldc = (K, N, N) if order == "r" else (M, K, M)
+        ca, cb = C.copy(), C.copy()
+        port.rdgemm(fold, order.encode(), b"n", b"n", M, N, K, 1.5, ptr(A), lda, ptr(B), ldb, 0.5, ptr(ca), ldc)
+        R.rdgemm(fold, order.encode(), b"n", b"n", M, N, K, 1.5, ptr(A), lda, ptr(B), ldb, 0.5, ptr(cb), ldc)
+        assert same_bits(ca, cb), ("rdgemm", order)
+
+
+@pytest.mark.parametrize("fold", [9, 21])
+def test_port_matches_reference_high_folds_fp32(port, fold):
+    """Folds above 8 up to binned_SBMAXFOLD (FP32 / float complex)."""
+    R = ref()
+    if R is None:
+        pytest.skip("reference library not built")
+    rng = np.random.default_rng(fold)
+    n = 4001
+    x = (np.exp2(rng.uniform(-100, 100, n)) * rng.choice([-1.0, 1.0], n)).astype(np.float32)
+    y = rng.standard_normal(n).astype(np.float32)
+    for name, args in (("sbssum", (ptr(x), 1)), ("sbsasum", (ptr(x), 1)),
+                       ("sbsdot", (ptr(x), 1, ptr(y), 1))):
+        a, b = binned_zeros(fold, "s"), binned_zeros(fold, "s")
+        getattr(port, name)(fold, n, *args, ptr(a))
+        getattr(R, name)(fold, n, *args, ptr(b))
+        assert same_state(a, b, fold), (name, fold)
+    a, b = binned_zeros(fold, "s"), binned_zeros(fold, "s")
+    assert port.sbsssq(fold, n, ptr(x), 1, 0.0, ptr(a)) == R.sbsssq(fold, n, ptr(x), 1, 0.0, ptr(b))
+    assert same_bits(a, b)
+    xc = (x + 1j * np.roll(y, 3)).astype(np.complex64)
+    a, b = binned_zeros(fold, "c"), binned_zeros(fold, "c")
+    port.cbcsum(fold, n, ptr(xc), 1, ptr(a))
+    R.cbcsum(fold, n, ptr(xc), 1, ptr(b))
+    assert same_state(a, b, fold, comps=2)
+    # float-complex dots: calls of at most 256 elements (where the reference stays canonical)
+    yc = (y - 1j * np.roll(x, 2)).astype(np.complex64)
+    for name in ("cbcdotc", "cbcdotu"):
+        a, b = binned_zeros(fold, "c"), binned_zeros(fold, "c")
+        for off in range(0, 1024, 256):
+            getattr(port, name)(fold, 256, ptr(xc[off:]), 1, ptr(yc[off:]), 1, ptr(a))
+            getattr(R, name)(fold, 256, ptr(xc[off:]), 1, ptr(yc[off:]), 1, ptr(b))
+        assert same_state(a, b, fold, comps=2), name
+
+
+def _ssq_random_tree(R, fold, x, rng):
+    """[scale, state] of x as the reference's binned_dbdbaddsq merges them over uneven chunks
+    in a random pairwise order."""
+    n = len(x)
+    nch = int(rng.integers(2, 200))
+    cuts = np.sort(rng.choice(np.arange(1, n), nch - 1, replace=False))
+    bounds = np.concatenate([[0], cuts, [n]])
+    parts = []
+    for i in range(nch):
+        z = binned_zeros(fold)
+        s = R.dbdssq(fold, int(bounds[i + 1] - bounds[i]), ptr(x[bounds[i]:]), 1, 0.0, ptr(z))
+        parts.append((s, z))
+    while len(parts) > 1:
+        i, j = (int(v) for v in rng.choice(len(parts), 2, replace=False))
+        (si, zi), (sj, zj) = parts[i], parts[j]
+        zj = zj.copy()
+        s = R.dbdbaddsq(fold, si, ptr(zi), sj, ptr(zj))
+        parts = [p for k, p in enumerate(parts) if k not in (i, j)] + [(s, zj)]
+    return parts[0]
+
+
+def test_reference_ssq_order_dependence_at_high_folds():
+    """A property of the reference itself: its scaled sum of squares (dmdssq with
+    binned_dmdrescale, merged by binned_dbdbaddsq as binnedMPI's DBDBADDSQ does) is
+    decomposition-invariant while the binned window stays above the subnormal range, but not
+    at high folds on values spanning a wide exponent range: there dmdrescale divides
+    primaries that have reached subnormal magnitudes, which rounds, so the state depends on
+    when each rescale happens. Random merge trees of the same data all agree with the single
+    call at fold 16 and do not at fold 52 (FP64; for FP32 the same holds from fold 11). The
+    GPU tests of the sums of squares at such folds use values whose reference result is
+    decomposition-invariant."""
+    R = ref()
+    if R is None:
+        pytest.skip("reference library not built")
+    x = gen("loguniform", 30001, 7)
+    rng = np.random.default_rng(1)
+    for fold, invariant in ((16, True), (52, False)):
+        w = binned_zeros(fold)
+        sw = R.dbdssq(fold, len(x), ptr(x), 1, 0.0, ptr(w))
+        same = []
+        for _ in range(6):
+            s, z = _ssq_random_tree(R, fold, x, rng)
+            same.append(s == sw and z.tobytes() == w.tobytes())
+        assert all(same) if invariant else not all(same), (fold, same)

@@ -228,7 +228,7 @@ def test_xblas23_errors(cuda, rb):
     rb.call("reproBLAS_rsgemv", 3, "r", "n", 0, 4, 1.0, A, 4, A, 1, 0.5, y, 1)
     assert (y.cpu().numpy() == 7.0).all()
     with pytest.raises(rb.ReproBLASError):
-        rb.call("reproBLAS_rsgemv", 9, "r", "n", 4, 4, 1.0, A, 4, A, 1, 0.5, y, 1)
+        rb.call("reproBLAS_rsgemv", 22, "r", "n", 4, 4, 1.0, A, 4, A, 1, 0.5, y, 1)   # above binned_SBMAXFOLD
     with pytest.raises(rb.ReproBLASError):
         rb.call("reproBLAS_rsgemv", 3, "r", "n", 4, 4, 1.0, A, 2, A, 1, 0.5, y, 1)
     one = np.array([1.0, 0.0], np.float32)
