@@ -352,16 +352,51 @@ struct GemmCfg {
   static constexpr int BK = 32;
 };
 
+// Upper bound of every magnitude whose 32-bit key (BT<double>::key: high word, sign cleared)
+// is at most k: the largest double with that high word.
+__device__ __forceinline__ double key_ceiling(unsigned k) {
+  return __longlong_as_double((long long)(((unsigned long long)k << 32) | 0xffffffffull));
+}
+
+// Shared-memory row of TN (1, 2 or 4) adjacent doubles, 16-byte aligned when TN > 1.
+template <int TN>
+__device__ __forceinline__ void lds_row(const double* p, double (&v)[TN]) {
+  if constexpr (TN == 1) {
+    v[0] = p[0];
+  } else {
+#pragma unroll
+    for (int t = 0; t < TN; t += 2) {
+      const double2 w = *(const double2*)(p + t);
+      v[t] = w.x;
+      v[t + 1] = w.y;
+    }
+  }
+}
+
 // One BM x BN tile of C at (m0, n0), computed by the 256 threads of the calling CTA (the
-// caller must keep the whole CTA in step: the tile uses __syncthreads).
+// caller must keep the whole CTA in step: the tile uses __syncthreads). Thread (tx, ty) owns
+// the TM x TN entries at rows ty*TM.. and columns tx*TN.. of the tile, so that its operands
+// sit next to each other in the shared tiles and load as 16-byte vectors.
+//
+// Per K tile the CTA records the largest-magnitude key of every row of op(A) and column of
+// op(B) in it (a warp-wide max per row / column). When, for every entry of a thread, the
+// product of the two magnitude bounds stays below the entry's cap and the tile's deposits fit
+// the endurance, no product of the tile can need an index raise, a renormalisation or a
+// non-finite branch: the tile's products are deposited without per-product checks, exactly
+// as the per-step fast path (tileN) would deposit them. Otherwise the tile takes the
+// per-step path. Both give the same state.
 template <int F, int TM, int TN>
 __device__ __forceinline__ void gemm_tile(const GemmArgs& g, long long m0, long long n0) {
   using Cfg = GemmCfg<F, TM, TN>;
+  using B = BT<double>;
   constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK;
-  __shared__ double As[BK][BM + 1];
-  __shared__ double Bs[BK][BN + 1];
-  const int tid = threadIdx.x;
+  constexpr int LDA = BM + 2, LDB = BN + 2;   // even strides: rows stay 16-byte aligned
+  __shared__ __align__(16) double As[BK][LDA];
+  __shared__ __align__(16) double Bs[BK][LDB];
+  __shared__ unsigned rowkey[BM], colkey[BN];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int tx = tid % Cfg::TX, ty = tid / Cfg::TX;
+  const int ra = ty * TM, cb = tx * TN;   // this thread's first row / column in the tile
 
   Acc<double, F> acc[TM * TN];   // entry (i, j) at i * TN + j
 #pragma unroll
@@ -396,27 +431,60 @@ __device__ __forceinline__ void gemm_tile(const GemmArgs& g, long long m0, long 
       Bs[k][j] = v;
     }
     __syncthreads();
-    const int kmax = (g.K - k0) < BK ? (int)(g.K - k0) : BK;
-    // past K both tiles hold zeros, whose products deposit nothing
+    // largest key of each row of the A tile and each column of the B tile (lane = k)
 #pragma unroll 1
-    for (int kk = 0; kk < BK; kk += 4) {
-      if (kk >= kmax) break;
-      double av[TM][4], bv[TN][4];
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-#pragma unroll
-        for (int i = 0; i < TM; i++) av[i][q] = As[kk + q][ty + i * Cfg::TY];
-#pragma unroll
-        for (int j = 0; j < TN; j++) bv[j][q] = Bs[kk + q][tx + j * Cfg::TX];
+    for (int r = warp; r < BM + BN; r += 8) {
+      const double v = r < BM ? As[lane][r] : Bs[lane][r - BM];
+      const unsigned m = __reduce_max_sync(0xffffffffu, B::key(v));
+      if (lane == 0) {
+        if (r < BM) rowkey[r] = m;
+        else colkey[r - BM] = m;
       }
-      double p[TM * TN][4];
+    }
+    __syncthreads();
+    const int kmax = (g.K - k0) < BK ? (int)(g.K - k0) : BK;
+    const int kend = (kmax + 3) & ~3;   // whole steps of 4; past K both tiles hold zeros
+    bool fast = true;
 #pragma unroll
-      for (int i = 0; i < TM; i++)
+    for (int i = 0; i < TM; i++) {
+      const double au = key_ceiling(rowkey[ra + i]);
 #pragma unroll
-        for (int j = 0; j < TN; j++)
+      for (int j = 0; j < TN; j++) {
+        const unsigned bound = B::key(__dmul_rn(au, key_ceiling(colkey[cb + j])));
+        fast = fast && acc[i * TN + j].fast(bound, kend);
+      }
+    }
+    if (fast) {
 #pragma unroll
-          for (int q = 0; q < 4; q++) p[i * TN + j][q] = __dmul_rn(av[i][q], bv[j][q]);
-      tileN<double, F, 4, TM * TN>(acc, p);
+      for (int e = 0; e < TM * TN; e++) acc[e].deposits += kend;
+#pragma unroll 1
+      for (int kk = 0; kk < kend; kk += 4) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          double av[TM], bv[TN];
+          lds_row<TM>(&As[kk + q][ra], av);
+          lds_row<TN>(&Bs[kk + q][cb], bv);
+#pragma unroll
+          for (int i = 0; i < TM; i++)
+#pragma unroll
+            for (int j = 0; j < TN; j++) acc[i * TN + j].deposit(__dmul_rn(av[i], bv[j]));
+        }
+      }
+    } else {
+      // per-step path, one entry at a time (the state does not depend on the interleaving;
+      // keeping few products live leaves the registers to the path above)
+#pragma unroll 1
+      for (int kk = 0; kk < kend; kk += 4) {
+#pragma unroll
+        for (int i = 0; i < TM; i++)
+#pragma unroll
+          for (int j = 0; j < TN; j++) {
+            double p[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) p[q] = __dmul_rn(As[kk + q][ra + i], Bs[kk + q][cb + j]);
+            acc[i * TN + j].template tile<4>(p, 4);
+          }
+      }
     }
     __syncthreads();
   }
@@ -425,7 +493,7 @@ __device__ __forceinline__ void gemm_tile(const GemmArgs& g, long long m0, long 
   for (int i = 0; i < TM; i++)
 #pragma unroll
     for (int j = 0; j < TN; j++) {
-      const long long gi = m0 + ty + i * Cfg::TY, gj = n0 + tx + j * Cfg::TX;
+      const long long gi = m0 + ra + i, gj = n0 + cb + j;
       if (gi < g.M && gj < g.N) {
         acc[i * TN + j].renorm();
         const long long off = gi * g.sci + gj * g.scj;

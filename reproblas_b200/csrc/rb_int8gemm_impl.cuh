@@ -37,9 +37,16 @@ constexpr int BK = 32;          // K bytes per pipeline stage (one MMA K step)
 constexpr int kThreads = 320;   // warps 0-7 epilogue, warp 8 TMA producer, warp 9 MMA issuer
 constexpr int kMaxSlices = 12;
 
-// Columns per tile (and per accumulator): S accumulators of BN columns must fit the 512
-// TMEM columns.
-__host__ __device__ constexpr int tile_bn(int S) { return S <= 8 ? 64 : 32; }
+// Columns per tile (and per accumulator). The S accumulators of a CTA take S*BN TMEM
+// columns; at most 256 of them lets two CTAs share an SM's 512 columns, so that one CTA's
+// epilogue (TMEM -> binned FP64) overlaps the other's MMAs.
+__host__ __device__ constexpr int tile_bn(int S) { return S <= 4 ? 64 : 32; }
+// CTAs that share an SM: two when their accumulators take at most 256 TMEM columns each and
+// a ring of at least two stages (S * (128 + BN) * 32 bytes each) fits in half the shared
+// memory; else one
+__host__ __device__ constexpr int ctas_per_sm(int S) {
+  return (S * tile_bn(S) <= 256 && 2 * S * (128 + tile_bn(S)) * 32 <= 100 * 1024) ? 2 : 1;
+}
 
 // Largest K chunk whose int32 accumulators stay exact: (t+1) digit pairs of at most
 // 127^2 per K index, t < S.
@@ -243,7 +250,10 @@ __host__ __device__ constexpr uint32_t stage_bytes() {
 }
 template <int S>
 __host__ __device__ constexpr int num_stages() {
-  return (200 * 1024) / (int)stage_bytes<S>() > 6 ? 6 : (200 * 1024) / (int)stage_bytes<S>();
+  // a ring of at most 6 stages in the CTA's share of the 227 KB of shared memory
+  return (200 * 1024 / ctas_per_sm(S)) / (int)stage_bytes<S>() > 6
+             ? 6
+             : (200 * 1024 / ctas_per_sm(S)) / (int)stage_bytes<S>();
 }
 template <int S>
 __host__ __device__ constexpr int tmem_cols() {
@@ -259,7 +269,7 @@ __host__ __device__ constexpr size_t dyn_smem_bytes() {
 // so A slice p starts at p*128*16 (LBO = S*128*16 between the two K halves) and the B
 // slices are stacked along N (a run of nq slices from q0 is one operand of nq*BN rows).
 template <int S, int F>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads, ctas_per_sm(S))
 gemm_i8_kernel(GemmI8Args g, const __grid_constant__ CUtensorMap tmA,
                const __grid_constant__ CUtensorMap tmB) {
   constexpr int BN = tile_bn(S);
@@ -394,7 +404,7 @@ gemm_i8_kernel(GemmI8Args g, const __grid_constant__ CUtensorMap tmA,
 
   // ---- epilogue: warp w reads TMEM lanes 32(w%4)..+31 (rows m0 + 32(w%4) + lane) and the
   // columns of half w/4 of the tile ----
-  constexpr int CW = S <= 8 ? 8 : 4;   // accumulator columns per TMEM load
+  constexpr int CW = S <= 4 ? 8 : 4;   // accumulator columns per TMEM load (fewer registers)
   if (ok && warp < 8) {
     const int quad = warp & 3, half = warp >> 2;
     const long long row = m0 + quad * 32 + lane;
