@@ -403,6 +403,9 @@ def headline(sec):
         return None
     h = {"dgemm_plain_tflops": {k: sec[k]["tflops"] for k in ("dgemm_plain_2048", "dgemm_plain_8192")
                                 if k in sec}}
+    if "fp64_probe" in sec:
+        h["dgemm_ceiling_tflops"] = sec["fp64_probe"]["dgemm_ceiling_tflops"]
+        h["fp64_add_tops"] = sec["fp64_probe"]["fp64_add_tops"]
     i8 = {}
     for S in (6, 7, 8, 10):
         r = sec.get("dgemm_int8_8192_s%d" % S)
@@ -618,6 +621,26 @@ def batched_case(torch, rb, rng, profile_steps=0, total_log2=28):
             "spot_check_bit_identical": bool(same)}
 
 
+def fp64_probe(torch, rb):
+    """The FP64 rates that bound the plain binned dgemm, measured on this GPU: independent
+    FP64 adds (the pipe's peak) and fl(a*b) products deposited into register-resident fold-3
+    accumulators (rb_probe_launch kinds 0 and 1; CUDA-event time, best of 3)."""
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    res = {}
+    for kind, iters, per in ((0, 1 << 16, 8), (1, 1 << 15, 4)):
+        grid = sms * max(1, rb.lib.rb_probe_occupancy(kind))
+        out = torch.empty(grid * 256, dtype=torch.float64, device="cuda")
+        stream = torch.cuda.current_stream().cuda_stream
+        run = lambda: rb.call("rb_probe_launch", kind, iters, grid, out, stream)
+        best = min(_event_time(torch, run, 1, warm=1) for _ in range(3))
+        res[kind] = grid * 256.0 * iters * per / best
+    return {"fp64_add_tops": round(res[0] / 1e12, 2),
+            "binned_products_per_s_T": round(res[1] / 1e12, 3),
+            "dgemm_ceiling_tflops": round(2 * res[1] / 1e12, 3),
+            "note": "ceiling = 2 flops x the rate of fl(a*b) deposited into fold-3 accumulators "
+                    "held in registers (no memory traffic); FP64 pipe peak for comparison"}
+
+
 def secondary(args):
     """dgemm TFLOP/s, plain binned vs int8-sliced (the second half of the headline metric),
     and dgemv GB/s; rank 0 at N=1. Device-resident operands, CUDA-event timing."""
@@ -640,8 +663,11 @@ def secondary(args):
     C = C0.clone()
     t = _event_time(torch, lambda: rb.call("reproBLAS_rdgemm", 3, "r", "n", "n", n, n, n, 1.5, A, n, B, n,
                                            0.5, C, n), 3)
+    out["fp64_probe"] = fp64_probe(torch, rb)
     out["dgemm_plain_2048"] = {"tflops": round(2 * n ** 3 / t / 1e12, 4), "ms": round(t * 1e3, 3),
-                               "bound": "fp64 pipe (binned deposit per product)"}
+                               "bound": "fp64 pipe (binned deposit per product)",
+                               "frac_of_deposit_ceiling": round(2 * n ** 3 / t / 1e12 /
+                                                                out["fp64_probe"]["dgemm_ceiling_tflops"], 3)}
     del A, B, C, C0
     # 8192^3: plain binned vs int8-sliced on the int8 configuration's data
     n = 8192

@@ -579,6 +579,16 @@ int rb_ddot_noalloc(const int fold, const int N, const double *X, const int incX
                     const double *Y, const int incY, double_binned *Z, double *result,
                     void *stream);
 
+/* Measurement kernels (no reference counterpart): the FP64 rates that bound the binned
+ * dgemm. kind 0: 8 * iters independent FP64 adds per thread; kind 1: 4 * iters products
+ * fl(a*b) per thread deposited into four register-resident fold-3 accumulators (the plain
+ * dgemm's unchecked tile loop without its memory traffic). `grid` CTAs of 256 threads, one
+ * double per thread written to the device array `out`, enqueued on `stream`; the caller times
+ * it. iters: a positive multiple of 8. rb_probe_occupancy: CTAs per SM of that kernel. */
+int rb_probe_launch(const int kind, const long long iters, const int grid, double *out,
+                    void *stream);
+int rb_probe_occupancy(const int kind);
+
 /* Library version string. */
 const char *rb_version(void);
 

@@ -115,6 +115,8 @@ SIGNATURES = {
     "rb_set_launch_config": (None, [_c_int, _c_int]),
     "rb_kernel_launch_count": (ctypes.c_ulonglong, []),
     "rb_synchronize": (_c_int, []),
+    "rb_probe_launch": (_c_int, [_c_int, _c_ll, _c_int, _c_vp, _c_vp]),
+    "rb_probe_occupancy": (_c_int, [_c_int]),
     "rb_debug_fail_allocations": (None, [_c_int]),
     "rb_debug_pipeline_fault": (None, [_c_ll, _c_ll]),
     "rb_version": (ctypes.c_char_p, []),

@@ -291,7 +291,20 @@ gemm_i8_kernel(GemmI8Args g, const __grid_constant__ CUtensorMap tmA,
   // 1024-byte aligned base for the stages
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const long long m0 = (long long)blockIdx.y * BM, n0 = (long long)blockIdx.x * BN;
+  // Tile order: groups of kGroupRows row blocks, column by column inside a group, so that the
+  // CTAs resident at one time share few A and B tiles (the slice arrays exceed the L2 at the
+  // large sizes). Every tile is independent, so the order changes no bit.
+  long long m0, n0;
+  {
+    constexpr int kGroupRows = 8;
+    const long long nx = gridDim.x, ny = gridDim.y;
+    const long long bid = (long long)blockIdx.y * nx + blockIdx.x;
+    const long long grp = bid / (kGroupRows * nx), first = grp * kGroupRows;
+    const long long rows = ny - first < kGroupRows ? ny - first : kGroupRows;
+    const long long in = bid - grp * kGroupRows * nx;
+    m0 = (first + in % rows) * BM;
+    n0 = (in / rows) * BN;
+  }
   const int nk = (int)(g.Kp / BK);
 
   if (tid == 0) {

@@ -35,7 +35,9 @@ def test_raw_accumulators_exact(cuda, rb, S):
     M, N, K = 200, 100, 300
     A = baseline_operands(rng, M, K)
     B = baseline_operands(rng, K, N)
-    Mp, Np, Kp = rup(M, 128), rup(N, 64 if S <= 8 else 32), rup(K, 32)
+    # B's rows are padded to the kernel's tile width: 64 columns up to 4 slices, else 32
+    # (tile_bn in rb_int8gemm_impl.cuh)
+    Mp, Np, Kp = rup(M, 128), rup(N, 64 if S <= 4 else 32), rup(K, 32)
     raw = cuda.zeros(S * Mp * Np, dtype=cuda.int32, device="cuda")
     As = cuda.zeros(S * Mp * Kp, dtype=cuda.int8, device="cuda")
     Bs = cuda.zeros(S * Np * Kp, dtype=cuda.int8, device="cuda")
