@@ -17,7 +17,10 @@ seeded). Prints ONE JSON line on rank 0.
   cpu_baseline  the ReproBLAS reference library (oracle/_ref, compiled from its own
           sources) on this host's cores: contiguous chunks, one thread each calling
           binnedBLAS_dbddot, merged with binned_dbdbadd (the reference's own MPI pattern),
-          bit-identical to the single call.
+          bit-identical to the single call (best of 5); one_core: reproBLAS_rddot exactly
+          as shipped, single-threaded (best of 5).
+  headline  last on the line: the dgemm half of the metric (plain vs int8-sliced TFLOP/s,
+          error over binned_dbbound), the measured deposit ceiling, dgemv and batched.
 
 --impl reference times that reference CPU path alone (rank 0; other ranks exit).
 Multi-GPU (torchrun, --gpus N): weak scaling, each rank reduces its own 2^28 shard; the
