@@ -352,6 +352,10 @@ struct GemmCfg {
   static constexpr int BK = 32;
 };
 
+// Reductions longer than this use the per-K-tile magnitude bound in gemm_tile (shorter ones,
+// e.g. the batched form's small instances, gain less than the bound's pass costs).
+constexpr long long kBoundMinK = 256;
+
 // Upper bound of every magnitude whose 32-bit key (BT<double>::key: high word, sign cleared)
 // is at most k: the largest double with that high word.
 __device__ __forceinline__ double key_ceiling(unsigned k) {
@@ -431,27 +435,32 @@ __device__ __forceinline__ void gemm_tile(const GemmArgs& g, long long m0, long 
       Bs[k][j] = v;
     }
     __syncthreads();
-    // largest key of each row of the A tile and each column of the B tile (lane = k)
-#pragma unroll 1
-    for (int r = warp; r < BM + BN; r += 8) {
-      const double v = r < BM ? As[lane][r] : Bs[lane][r - BM];
-      const unsigned m = __reduce_max_sync(0xffffffffu, B::key(v));
-      if (lane == 0) {
-        if (r < BM) rowkey[r] = m;
-        else colkey[r - BM] = m;
-      }
-    }
-    __syncthreads();
     const int kmax = (g.K - k0) < BK ? (int)(g.K - k0) : BK;
     const int kend = (kmax + 3) & ~3;   // whole steps of 4; past K both tiles hold zeros
-    bool fast = true;
+    // Long reductions (the bound pays for its pass and barrier): largest key of each row of
+    // the A tile and each column of the B tile (lane = k), then the entries' bounds. g.K is
+    // the same for the whole CTA.
+    bool fast = false;
+    if (g.K > kBoundMinK) {
+#pragma unroll 1
+      for (int r = warp; r < BM + BN; r += 8) {
+        const double v = r < BM ? As[lane][r] : Bs[lane][r - BM];
+        const unsigned m = __reduce_max_sync(0xffffffffu, B::key(v));
+        if (lane == 0) {
+          if (r < BM) rowkey[r] = m;
+          else colkey[r - BM] = m;
+        }
+      }
+      __syncthreads();
+      fast = true;
 #pragma unroll
-    for (int i = 0; i < TM; i++) {
-      const double au = key_ceiling(rowkey[ra + i]);
+      for (int i = 0; i < TM; i++) {
+        const double au = key_ceiling(rowkey[ra + i]);
 #pragma unroll
-      for (int j = 0; j < TN; j++) {
-        const unsigned bound = B::key(__dmul_rn(au, key_ceiling(colkey[cb + j])));
-        fast = fast && acc[i * TN + j].fast(bound, kend);
+        for (int j = 0; j < TN; j++) {
+          const unsigned bound = B::key(__dmul_rn(au, key_ceiling(colkey[cb + j])));
+          fast = fast && acc[i * TN + j].fast(bound, kend);
+        }
       }
     }
     if (fast) {
@@ -471,19 +480,22 @@ __device__ __forceinline__ void gemm_tile(const GemmArgs& g, long long m0, long 
         }
       }
     } else {
-      // per-step path, one entry at a time (the state does not depend on the interleaving;
-      // keeping few products live leaves the registers to the path above)
+      // per-step path: the key max of every entry's 4 products; when all entries are on
+      // their fast path the deposit chains are interleaved (tileN)
 #pragma unroll 1
       for (int kk = 0; kk < kend; kk += 4) {
+        double p[TM * TN][4];
 #pragma unroll
-        for (int i = 0; i < TM; i++)
+        for (int q = 0; q < 4; q++) {
+          double av[TM], bv[TN];
+          lds_row<TM>(&As[kk + q][ra], av);
+          lds_row<TN>(&Bs[kk + q][cb], bv);
 #pragma unroll
-          for (int j = 0; j < TN; j++) {
-            double p[4];
+          for (int i = 0; i < TM; i++)
 #pragma unroll
-            for (int q = 0; q < 4; q++) p[q] = __dmul_rn(As[kk + q][ra + i], Bs[kk + q][cb + j]);
-            acc[i * TN + j].template tile<4>(p, 4);
-          }
+            for (int j = 0; j < TN; j++) p[i * TN + j][q] = __dmul_rn(av[i], bv[j]);
+        }
+        tileN<double, F, 4, TM * TN>(acc, p);
       }
     }
     __syncthreads();
