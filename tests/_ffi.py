@@ -96,6 +96,7 @@ _SIGS = {
     "sindex": (c_int, [c_float]),
     "sbsbadd": (None, [c_int, c_vp, c_vp]),
     "ssbconv": (c_float, [c_int, c_vp]),
+    "ssmconv": (c_float, [c_int, c_vp, c_int, c_vp, c_int]),
 }
 
 # gemv / gemm of FP32 real (scalars by value) and complex (scalars by pointer) elements
@@ -141,7 +142,7 @@ _REF_NAMES = {
     "dbdbadd": "binned_dbdbadd", "dbdconv": "binned_dbdconv", "ddbconv": "binned_ddbconv", "ddmconv": "binned_ddmconv",
     "dbdbaddsq": "binned_dbdbaddsq", "dbbound": "binned_dbbound", "dscale": "binned_dscale",
     "dindex": "binned_dindex", "sindex": "binned_sindex", "sbsbadd": "binned_sbsbadd",
-    "ssbconv": "binned_ssbconv",
+    "ssbconv": "binned_ssbconv", "ssmconv": "binned_ssmconv",
     "sbsconv": "binned_sbsconv", "zbzconv": "binned_zbzconv", "cbcconv": "binned_cbcconv",
     "zbzbadd": "binned_zbzbadd", "cbcbadd": "binned_cbcbadd", "sbsbaddsq": "binned_sbsbaddsq",
 }

@@ -1,5 +1,6 @@
-"""BLAS1 sweep parity at full size: dsum, ddot, dnrm2 (FP64), ssum, sdot (FP32), zsum,
-zdotc (complex128) at N = 2^10, 2^12, ..., 2^28 elements, folds 2, 3 and 4, for uniform,
+"""BLAS1 sweep parity at full size: dsum, ddot, dnrm2, dasum (FP64), ssum, sdot, snrm2, sasum
+(FP32), zsum, zdotc, zdotu, dznrm2, dzasum (complex128), csum, scnrm2, scasum (complex64) at
+N = 2^10, 2^12, ..., 2^28 elements, folds 2, 3 and 4, for uniform,
 normal, log-uniform and ill-conditioned inputs. Every GPU result (binned state, the
 sum-of-squares scale, and the converted value of the reproBLAS_r* call) must equal the
 reference library bit for bit, and the largest N must give the same bits under 8 grid/block
@@ -19,8 +20,9 @@ import pytest
 
 from _cmp import same_state, same_value
 from _ffi import host_threads, port, ref
-from _sweep import (DISTS, FOLDS, GROUPS, KIND, LAUNCH_CONFIGS, LOGN, NMAX, gpu_call, gpu_state,
+from _sweep import (DISTS, FOLDS, GROUPS, LAUNCH_CONFIGS, LOGN, NMAX, SSQ, gpu_call, gpu_state,
                     group_inputs, reference_prefixes)
+from _sweep import comps as sweep_comps
 
 pytestmark = pytest.mark.gpu
 
@@ -35,7 +37,7 @@ def test_blas1_sweep_bit_exact(cuda, rb, dist, group):
     with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), host_threads()))) as ex:
         futs = {(r, f): ex.submit(reference_prefixes, L, r, f, x, y) for r, f in jobs}
         X = cuda.from_numpy(x).cuda()
-        Y = cuda.from_numpy(y).cuda()
+        Y = cuda.from_numpy(y).cuda() if y is not None else None
         got, got_cfg = {}, {}
         for r, f in jobs:
             for lg in LOGN:
@@ -52,16 +54,16 @@ def test_blas1_sweep_bit_exact(cuda, rb, dist, group):
     bad = []
     for (r, f, lg), (st, scl, val) in got.items():
         wst, wscl, wval = want[(r, f)][lg]
-        comps = 2 if KIND[r][0] == "z" else 1
+        comps = sweep_comps(r)
         if not same_state(st, wst, f, comps):
             bad.append((r, f, lg, "state"))
-        if r == "dnrm2" and scl != wscl:
+        if r in SSQ and scl != wscl:
             bad.append((r, f, lg, "scale", scl, wscl))
         if not same_value(val, wval):
             bad.append((r, f, lg, "value", val, wval))
     for (r, f, cps, thr), (st, scl) in got_cfg.items():
         wst, wscl, _ = want[(r, f)][LOGN[-1]]
-        comps = 2 if KIND[r][0] == "z" else 1
-        if not same_state(st, wst, f, comps) or (r == "dnrm2" and scl != wscl):
+        comps = sweep_comps(r)
+        if not same_state(st, wst, f, comps) or (r in SSQ and scl != wscl):
             bad.append((r, f, "launch", cps, thr))
     assert not bad, (dist, group, "reference" if ref() else "oracle", bad[:10])

@@ -7,7 +7,8 @@ import pytest
 
 from _cmp import same_state, same_value
 from _ffi import ref
-from _sweep import DISTS, FOLDS, GROUPS, KIND, group_inputs, reference_prefixes
+from _sweep import DISTS, FOLDS, GROUPS, SSQ, group_inputs, reference_prefixes
+from _sweep import comps as sweep_comps
 
 LOGN_SMALL = [10, 12, 14, 16]
 
@@ -19,7 +20,7 @@ def test_prefix_pass_equals_single_calls(port, dist, group):
     R = ref()
     libs = [port] + ([R] if R is not None else [])
     for r in GROUPS[group]:
-        comps = 2 if KIND[r][0] == "z" else 1
+        comps = sweep_comps(r)
         for f in FOLDS:
             passes = []
             for L in libs:
