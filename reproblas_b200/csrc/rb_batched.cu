@@ -106,8 +106,7 @@ __device__ __forceinline__ void warp_segment(const Args& a, int s) {
     acc.template tile<K>(v, nv);
   }
   acc.renorm();
-#pragma unroll 1
-  for (int m = 16; m; m >>= 1) acc.merge(acc.shfl_xor(m));
+  warp_merge_all(acc);
   if (lane == 0) finish_segment<F>(a, s, acc);
 }
 

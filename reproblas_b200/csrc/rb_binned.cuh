@@ -453,6 +453,56 @@ __device__ __forceinline__ void tileN(Acc<T, F> (&a)[N], const T (&v)[N][K]) {
   for (int n = 0; n < N; n++) a[n].template tile<K>(v[n], K);
 }
 
+// Merge the renormalised accumulators a[n] of the 32 lanes of a warp, for N accumulators at
+// once; every lane ends with the merged states (a butterfly). The lanes first move to the
+// warp's coarsest index (dmdupdate: the alignment merge() performs per pair, done once) and
+// an empty accumulator becomes the zero state at that index (its primaries the bins, its
+// carries 0: merging it changes nothing). Every pair merge is then merge()'s equal-index
+// branch, the same arithmetic and renormalisation, on the primaries and carries alone, and
+// the N chains are interleaved. The non-finite classes are OR-ed once.
+template <typename T, int F, int N>
+__device__ __forceinline__ void warp_merge_all(Acc<T, F> (&a)[N]) {
+  using B = BT<T>;
+  int m[N];
+  T bins[N][F];
+#pragma unroll
+  for (int n = 0; n < N; n++) {
+    a[n].flags = __reduce_or_sync(0xffffffffu, a[n].flags);
+    m[n] = __reduce_min_sync(0xffffffffu, a[n].idx);   // kEmpty is above every index
+    if (m[n] != kEmpty) {
+      if (a[n].idx == kEmpty) {
+#pragma unroll
+        for (int i = 0; i < F; i++) { a[n].pri[i] = B::bin(m[n] + i); a[n].car[i] = T(0); }
+        a[n].set_idx(m[n]);
+      } else if (a[n].idx > m[n]) {
+        a[n].raise_to(m[n]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < F; i++) bins[n][i] = B::bin(m[n] + i);
+  }
+#pragma unroll
+  for (int s = 16; s; s >>= 1) {
+#pragma unroll
+    for (int n = 0; n < N; n++) {
+      if (m[n] == kEmpty) continue;   // warp-uniform
+#pragma unroll
+      for (int i = 0; i < F; i++) {
+        const T p = __shfl_xor_sync(0xffffffffu, a[n].pri[i], s);
+        const T c = __shfl_xor_sync(0xffffffffu, a[n].car[i], s);
+        a[n].pri[i] = B::add(a[n].pri[i], B::sub(p, bins[n][i]));
+        a[n].car[i] = B::add(a[n].car[i], c);
+      }
+      a[n].renorm();
+    }
+  }
+}
+
+template <typename T, int F>
+__device__ __forceinline__ void warp_merge_all(Acc<T, F>& a) {
+  warp_merge_all<T, F, 1>(*reinterpret_cast<Acc<T, F>(*)[1]>(&a));
+}
+
 // binned_ddmconv (src/binned/ddmconv.c:23-81): fixed-order conversion to double with
 // scaling when the index is within 3 of the top. `F` is the fold (any fold; the template
 // form below serves the kernels of a fixed fold).

@@ -153,8 +153,7 @@ __global__ void __launch_bounds__(256) gemv_rows_kernel(GemvArgs g) {
     }
   }
   a.renorm();
-#pragma unroll 1
-  for (int m = 16; m; m >>= 1) a.merge(a.shfl_xor(m));
+  warp_merge_all(a);
   if (lane == 0) {
     double* rec = smem + warp * REC;
 #pragma unroll

@@ -80,11 +80,14 @@ __device__ __forceinline__ E convx(const E* p, const E* c, int inc) {
 }
 
 // Finish one output entry from the renormalised state of its products, a[0..NC-1]:
-// kOutValue starts from binned(beta*y) (nothing when beta == 0, binned(y) when beta == 1;
-// rzgemv.c:47-59) and writes the converted value over y; kOutBinned merges into the
-// caller's state (reference layout: NC-interleaved primaries, then carries).
+// kOutValue deposits beta*y into it (nothing when beta == 0, y itself when beta == 1;
+// rzgemv.c:47-59 starts from binned(beta*y) -- the same multiset, so the same state) and
+// writes the converted value to yout; yin holds y (read by the caller, possibly early).
+// kOutBinned merges into the caller's state (reference layout: NC-interleaved primaries,
+// then carries).
 template <typename E, bool CX, int F>
-__device__ __forceinline__ void finish(Acc<E, F>* a, int mode, E* yv, E br, E bi, E* yb) {
+__device__ __forceinline__ void finish_from(Acc<E, F>* a, int mode, const E* yin, E* yout, E br,
+                                            E bi, E* yb) {
   constexpr int NC = CX ? 2 : 1;
   using B = BT<E>;
   if (mode == kOutValue) {
@@ -92,7 +95,7 @@ __device__ __forceinline__ void finish(Acc<E, F>* a, int mode, E* yv, E br, E bi
     const bool bone = br == E(1) && (!CX || bi == E(0));
     E init[NC];
     if constexpr (CX) {
-      const E yr = yv[0], yi = yv[1];
+      const E yr = yin[0], yi = yin[1];
       if (bone) {
         init[0] = yr;
         init[1] = yi;
@@ -101,22 +104,18 @@ __device__ __forceinline__ void finish(Acc<E, F>* a, int mode, E* yv, E br, E bi
         init[1] = B::add(B::mul(yr, bi), B::mul(yi, br));
       }
     } else {
-      init[0] = bone ? yv[0] : B::mul(yv[0], br);
+      init[0] = bone ? yin[0] : B::mul(yin[0], br);
     }
 #pragma unroll
     for (int c = 0; c < NC; c++) {
-      Acc<E, F> t;
-      t.zero();
       if (!bzero) {
         E v[1] = {init[c]};
-        t.template tile<1>(v, 1);
-        t.renorm();
+        a[c].template tile<1>(v, 1);
       }
-      t.merge(a[c]);
-      t.renorm();
+      a[c].renorm();
       E p[F], q[F];
-      t.store(p, q, 1);
-      yv[c] = convx<E, F>(p, q, 1);
+      a[c].store(p, q, 1);
+      yout[c] = convx<E, F>(p, q, 1);
     }
   } else {
 #pragma unroll
@@ -128,6 +127,19 @@ __device__ __forceinline__ void finish(Acc<E, F>* a, int mode, E* yv, E br, E bi
       prev.store(yb + c, yb + NC * F + c, NC);
     }
   }
+}
+
+template <typename E, bool CX, int F>
+__device__ __forceinline__ void finish(Acc<E, F>* a, int mode, E* yv, E br, E bi, E* yb) {
+  constexpr int NC = CX ? 2 : 1;
+  E yin[NC];
+#pragma unroll
+  for (int c = 0; c < NC; c++) yin[c] = E(0);
+  if (mode == kOutValue) {
+#pragma unroll
+    for (int c = 0; c < NC; c++) yin[c] = yv[c];
+  }
+  finish_from<E, CX, F>(a, mode, yin, yv, br, bi, yb);
 }
 
 template <typename E>
@@ -279,6 +291,15 @@ __global__ void __launch_bounds__(256, (F <= 3 && !(CX && sizeof(E) == 8)) ? 3 :
     Acc<E, F> a[NC];
 #pragma unroll
     for (int q = 0; q < NC; q++) a[q].zero();
+    // y of the row, read now so that its latency overlaps the streaming (only the lane that
+    // may finish the row reads it)
+    E yin[NC];
+#pragma unroll
+    for (int q = 0; q < NC; q++) yin[q] = E(0);
+    if (g.mode == kOutValue && lane == 0) {
+#pragma unroll
+      for (int q = 0; q < NC; q++) yin[q] = g.y[r * g.incy * NC + q];
+    }
     const E* row = g.A + r * g.lda * NC;
     long long ce = c0;   // start of the element path
     if (g.vec) {
@@ -366,11 +387,8 @@ __global__ void __launch_bounds__(256, (F <= 3 && !(CX && sizeof(E) == 8)) ? 3 :
       deposit_tile<E, CX, F, K * D>(a, v, nv);
     }
 #pragma unroll
-    for (int q = 0; q < NC; q++) {
-      a[q].renorm();
-#pragma unroll 1
-      for (int m = 16; m; m >>= 1) a[q].merge(a[q].shfl_xor(m));
-    }
+    for (int q = 0; q < NC; q++) a[q].renorm();
+    warp_merge_all<E, F, NC>(a);
     bool done = c0 == 0 && c1 == g.C;   // the whole row is this warp's
     if (!done) {
       // part of a cut row: record in slot 2w (the warp's first row) or 2w+1 (its last row);
@@ -392,27 +410,37 @@ __global__ void __launch_bounds__(256, (F <= 3 && !(CX && sizeof(E) == 8)) ? 3 :
         long long fw = gwarp, lw = gwarp;
         while (fw > 0 && sp.start(fw) > rs) fw--;
         while (lw + 1 < nwe && sp.start(lw + 1) < re) lw++;
-        // lanes take the parts of warps fw + lane, fw + lane + 32, ...; then a butterfly
-#pragma unroll
-        for (int q = 0; q < NC; q++) a[q].zero();
+        if (lw - fw < 4) {
+          // a few parts (most often two: the row is cut once): every lane merges the other
+          // warps' records into its copy of this warp's part, which it holds already
 #pragma unroll 1
-        for (long long v = fw + lane; v <= lw; v += 32) {
-          const long long vs = sp.start(v) >= rs ? 2 * v : 2 * v + 1;
+          for (long long v = fw; v <= lw; v++) {
+            if (v == gwarp) continue;
+            const long long vs = sp.start(v) >= rs ? 2 * v : 2 * v + 1;
 #pragma unroll
-          for (int q = 0; q < NC; q++)
-            merge_rec<E, F, true>(a[q], g.scratch + vs * REC + q * (2 * F + 1), 1);
-        }
+            for (int q = 0; q < NC; q++)
+              merge_rec<E, F, true>(a[q], g.scratch + vs * REC + q * (2 * F + 1), 1);
+          }
+        } else {
+          // lanes take the parts of warps fw + lane, fw + lane + 32, ...; then a butterfly
 #pragma unroll
-        for (int q = 0; q < NC; q++) {
+          for (int q = 0; q < NC; q++) a[q].zero();
 #pragma unroll 1
-          for (int m = 16; m; m >>= 1) a[q].merge(a[q].shfl_xor(m));
+          for (long long v = fw + lane; v <= lw; v += 32) {
+            const long long vs = sp.start(v) >= rs ? 2 * v : 2 * v + 1;
+#pragma unroll
+            for (int q = 0; q < NC; q++)
+              merge_rec<E, F, true>(a[q], g.scratch + vs * REC + q * (2 * F + 1), 1);
+          }
+          warp_merge_all<E, F, NC>(a);
         }
         if (lane == 0) g.tickets[r] = 0u;
         done = true;
       }
     }
     if (done && lane == 0)
-      finish<E, CX, F>(a, g.mode, g.y + r * g.incy * NC, g.br, g.bi, g.ybin + r * g.incy * 2 * F * NC);
+      finish_from<E, CX, F>(a, g.mode, yin, g.y + r * g.incy * NC, g.br, g.bi,
+                            g.ybin + r * g.incy * 2 * F * NC);
     pos = (r + 1) * g.C;
   }
 }
