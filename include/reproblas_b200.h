@@ -464,12 +464,13 @@ rb_batch_plan *rb_batch_plan_create(const int fold, const int nseg, const long l
                                     const int *seg_lengths, const double *X, const double *Y,
                                     double *results, double_binned *states, const int ngemm,
                                     const rb_dgemm_instance *gemms);
-/* Tries every candidate schedule (gemm tile 16x16 / 32x32 / 32x64, long-segment chunk
+/* Tries every candidate schedule (gemm tile 16x16 / 32x32 / 32x64 / 16x32 / 32x16, chunk
  * length, short-segment threshold, CTAs per SM) from the plan's original outputs,
  * rejects any candidate whose output bits differ from the first candidate's, keeps the
  * fastest over `reps` timed launches, and restores the outputs. Synchronises the device. */
 int rb_batch_plan_autotune(rb_batch_plan *plan, const int reps);
-/* Sets the schedule explicitly (tile 0: 16x16, 1: 32x32, 2: 32x64 with fold <= 3). */
+/* Sets the schedule explicitly (tile 0: 16x16, 1: 32x32, 2: 32x64 with fold <= 3, 3: 16x32,
+   4: 32x16). */
 int rb_batch_plan_set_config(rb_batch_plan *plan, const int tile, const long long chunk,
                              const long long small_max, const int ctas_per_sm);
 /* Enqueues one execution (one graph launch of the single persistent kernel) on `stream`.

@@ -225,16 +225,21 @@ __global__ void count_diff_kernel(const unsigned long long* a, const unsigned lo
   if (c) atomicAdd(out, c);
 }
 
-// tile shapes the autotuner chooses from (TM x TN entries per thread, 16 x 16 threads)
-constexpr int kTileShapes = 3;
-__host__ __device__ constexpr int tile_tm(int t) { return t == 0 ? 1 : 2; }
-__host__ __device__ constexpr int tile_tn(int t) { return t == 2 ? 4 : (t == 0 ? 1 : 2); }
+// tile shapes the autotuner chooses from (TM x TN entries per thread, 16 x 16 threads):
+// 16x16, 32x32, 32x64 (folds up to 3), 16x32, 32x16
+constexpr int kTileShapes = 5;
+__host__ __device__ constexpr int tile_tm(int t) { return t == 0 || t == 3 ? 1 : 2; }
+__host__ __device__ constexpr int tile_tn(int t) {
+  return t == 2 ? 4 : (t == 0 || t == 4 ? 1 : 2);
+}
 
 template <int F>
 cudaError_t launch_batched(int tile, dim3 grid, const Args& a, cudaStream_t s) {
   switch (tile) {
     case 0: batched_kernel<F, 1, 1><<<grid, 256, 0, s>>>(a); break;
     case 1: batched_kernel<F, 2, 2><<<grid, 256, 0, s>>>(a); break;
+    case 3: batched_kernel<F, 1, 2><<<grid, 256, 0, s>>>(a); break;
+    case 4: batched_kernel<F, 2, 1><<<grid, 256, 0, s>>>(a); break;
     default:
       if constexpr (F <= 3) batched_kernel<F, 2, 4><<<grid, 256, 0, s>>>(a);
       else return cudaErrorInvalidValue;
@@ -248,6 +253,8 @@ const void* batched_ptr(int tile) {
   switch (tile) {
     case 0: return (const void*)batched_kernel<F, 1, 1>;
     case 1: return (const void*)batched_kernel<F, 2, 2>;
+    case 3: return (const void*)batched_kernel<F, 1, 2>;
+    case 4: return (const void*)batched_kernel<F, 2, 1>;
     default:
       if constexpr (F <= 3) return (const void*)batched_kernel<F, 2, 4>;
       else return nullptr;
@@ -553,7 +560,7 @@ int rb_batch_plan_set_config(rb_batch_plan* p, const int tile, const long long c
   using namespace rb;
   if (!p || tile < 0 || tile >= bt::kTileShapes || (tile == 2 && p->fold > 3) || chunk < 256 ||
       small_max < 0 || ctas_per_sm < 0) {
-    set_error(RB_ERR_INVALID_ARG, "rb_batch_plan_set_config: tile in [0, 2] (2 needs fold <= 3), "
+    set_error(RB_ERR_INVALID_ARG, "rb_batch_plan_set_config: tile in [0, 4] (2 needs fold <= 3), "
                                   "chunk >= 256, small_max >= 0, ctas_per_sm >= 0");
     return RB_ERR_INVALID_ARG;
   }

@@ -109,7 +109,7 @@ def test_batched_matches_per_instance_calls(cuda, rb):
         for got, want in zip(P.gemm_outputs(), want_c):
             assert got.tobytes() == want.tobytes()
         # every schedule gives the same bits
-        for tile in (0, 1, 2):
+        for tile in (0, 1, 2, 3, 4):
             for chunk, small in ((256, 0), (1 << 13, 512), (1 << 15, 1 << 20)):
                 P.reset_gemms()
                 P.results.zero_()
