@@ -591,7 +591,7 @@ int rb_batch_plan_autotune(rb_batch_plan* p, const int reps) {
   std::vector<Cand> cands;
   for (int t = 0; t < bt::kTileShapes; t++) {
     if (t == 2 && p->fold > 3) continue;
-    for (long long ch : {1ll << 13, 1ll << 14, 1ll << 16})
+    for (long long ch : {1ll << 13, 1ll << 14, 1ll << 16, 1ll << 18, 1ll << 20})
       for (long long sm : {512ll, 4096ll})
         for (int cps : {0, 2})
           cands.push_back({t, ch, sm, cps});
