@@ -425,10 +425,11 @@ int rb_dgemm_int8(const int fold, const char Order, const char TransA, const cha
                   const int ldc, const int nslices);
 
 /* Test hook for rb_dgemm_int8 (row-major, no transposes, alpha 1, fold 3): device outputs
- * raw[t][Mp][Np] = the int32 accumulators of digit-pair sums p + q = t (padded sizes
- * Mp = M rounded up to 128, Np = N rounded up to 64), the digit slices
- * as_out[p][Mp][Kp] / bs_out[q][Np][Kp] (Kp = K rounded up to 64, B transposed) and the
- * exponents ea_out[M] / fb_out[N]. Any output may be NULL except raw. */
+ * raw[t][Mp][Np] = the int32 accumulators of digit-pair sums p + q = t of the first K chunk
+ * (padded sizes Mp = M rounded up to 128, Np = N rounded up to the output tile width: 64 for
+ * up to 4 slices, 32 above), the digit slices as_out[p][Mp][Kp] / bs_out[q][Np][Kp] (Kp = the
+ * first K chunk rounded up to 32, B transposed) and the exponents ea_out[M] / fb_out[N]. Any
+ * output may be NULL except raw. */
 int rb_dgemm_int8_inspect(const int M, const int N, const int K, const double *A,
                           const double *B, const int nslices, int *raw, signed char *as_out,
                           signed char *bs_out, int *ea_out, int *fb_out);
