@@ -284,12 +284,11 @@ template <typename T> struct VecW;
 template <> struct VecW<double> { static constexpr int n = 2; };
 template <> struct VecW<float> { static constexpr int n = 4; };
 
-// The scaled sum of squares carries a scale next to its accumulator; the FP64 one is held to
-// four CTAs per SM (64 registers), which pays for a few spills, the FP32 one, which keeps the
-// next warp tile's loads in flight while it deposits the current one, to three. (A minimum of
-// 0 leaves the others to the compiler's own choice.)
+// The scaled sum of squares carries a scale next to its accumulator; it is held to four CTAs
+// per SM (64 registers), which pays for a few spills. (A minimum of 0 leaves the others to
+// the compiler's own choice.)
 template <typename T, int F, int OP, bool VEC>
-__global__ void __launch_bounds__(256, OP == kOpSsq ? (sizeof(T) == 4 ? 3 : 4) : 0)
+__global__ void __launch_bounds__(256, OP == kOpSsq ? 4 : 0)
 blas1_kernel(Blas1Args args) {
   constexpr int VW = VecW<T>::n;     // elements per 16-byte vector
   constexpr int NV = 4;              // vectors per thread per warp tile
@@ -312,37 +311,8 @@ blas1_kernel(Blas1Args args) {
     body_end = args.body_end;
     const long long nwt = (body_end - head) / WT;
     const long long gwarp = gtid >> 5, nwarps = nthreads >> 5;
-    // FP32 sum of squares: the deposits of a tile (a multiply more per element than ssum,
-    // at fewer warps per SM) outlast its loads, so the next tile is loaded first (two
-    // register buffers, used in turn)
-    constexpr bool kPrefetch = OP == kOpSsq && sizeof(T) == 4;
-    if (kPrefetch) {
-      auto load = [&](long long wt, T (&v)[NV * VW]) {
-        const long long base = head + wt * WT;
-#pragma unroll
-        for (int k = 0; k < NV; k++) {
-          T t[VW];
-          ldv(x + base + (long long)(k * 32 + lane) * VW, t);
-#pragma unroll
-          for (int j = 0; j < VW; j++) v[k * VW + j] = t[j];
-        }
-      };
-      T va[NV * VW], vb[NV * VW];
-      long long wt = gwarp;
-      if (wt < nwt) load(wt, va);
 #pragma unroll 1
-      while (wt < nwt) {
-        if (wt + nwarps < nwt) load(wt + nwarps, vb);
-        st.template tile<NV * VW>(va, va, NV * VW);
-        wt += nwarps;
-        if (wt >= nwt) break;
-        if (wt + nwarps < nwt) load(wt + nwarps, va);
-        st.template tile<NV * VW>(vb, vb, NV * VW);
-        wt += nwarps;
-      }
-    }
-#pragma unroll 1
-    for (long long wt = gwarp; !kPrefetch && wt < nwt; wt += nwarps) {
+    for (long long wt = gwarp; wt < nwt; wt += nwarps) {
       const long long base = head + wt * WT;
       T xv[NV * VW], yv[NV * VW];
 #pragma unroll
