@@ -407,31 +407,59 @@ __device__ __forceinline__ void gemm_tile(const GemmArgs& g, long long m0, long 
 
   const bool a_k_fast = g.sak == 1;   // which stride is unit decides the load order
   const bool b_j_fast = g.sbj == 1;
+  // whole tiles with a unit stride, an even leading dimension and a 16-byte aligned base
+  // load 16-byte pairs
+  const bool a_pairs = a_k_fast && (g.sai & 1) == 0 && ((uintptr_t)g.A & 15) == 0 && m0 + BM <= g.M;
+  const bool b_pairs = b_j_fast && (g.sbk & 1) == 0 && ((uintptr_t)g.B & 15) == 0 && n0 + BN <= g.N;
 
 #pragma unroll 1
   for (long long k0 = 0; k0 < g.K; k0 += BK) {
+    const bool k_whole = k0 + BK <= g.K;
     // A tile: BM x BK
+    if (a_pairs && k_whole) {
 #pragma unroll 1
-    for (int e = tid; e < BM * BK; e += 256) {
-      int i, k;
-      if (a_k_fast) { k = e % BK; i = e / BK; } else { i = e % BM; k = e / BM; }
-      const long long gi = m0 + i, gk = k0 + k;
-      double v = 0.0;
-      if (gi < g.M && gk < g.K) {
-        v = __ldg(g.A + gi * g.sai + gk * g.sak);
-        if (g.alpha != 1.0) v = __dmul_rn(v, g.alpha);
+      for (int e = tid; e < BM * BK / 2; e += 256) {
+        const int i = e / (BK / 2), k = 2 * (e % (BK / 2));
+        const double2 v = __ldg((const double2*)(g.A + (m0 + i) * g.sai + k0 + k));
+        double v0 = v.x, v1 = v.y;
+        if (g.alpha != 1.0) {
+          v0 = __dmul_rn(v0, g.alpha);
+          v1 = __dmul_rn(v1, g.alpha);
+        }
+        As[k][i] = v0;
+        As[k + 1][i] = v1;
       }
-      As[k][i] = v;
+    } else {
+#pragma unroll 1
+      for (int e = tid; e < BM * BK; e += 256) {
+        int i, k;
+        if (a_k_fast) { k = e % BK; i = e / BK; } else { i = e % BM; k = e / BM; }
+        const long long gi = m0 + i, gk = k0 + k;
+        double v = 0.0;
+        if (gi < g.M && gk < g.K) {
+          v = __ldg(g.A + gi * g.sai + gk * g.sak);
+          if (g.alpha != 1.0) v = __dmul_rn(v, g.alpha);
+        }
+        As[k][i] = v;
+      }
     }
     // B tile: BK x BN
+    if (b_pairs && k_whole) {
 #pragma unroll 1
-    for (int e = tid; e < BK * BN; e += 256) {
-      int k, j;
-      if (b_j_fast) { j = e % BN; k = e / BN; } else { k = e % BK; j = e / BK; }
-      const long long gk = k0 + k, gj = n0 + j;
-      double v = 0.0;
-      if (gk < g.K && gj < g.N) v = __ldg(g.B + gk * g.sbk + gj * g.sbj);
-      Bs[k][j] = v;
+      for (int e = tid; e < BK * BN / 2; e += 256) {
+        const int k = e / (BN / 2), j = 2 * (e % (BN / 2));
+        *(double2*)&Bs[k][j] = __ldg((const double2*)(g.B + (k0 + k) * g.sbk + n0 + j));
+      }
+    } else {
+#pragma unroll 1
+      for (int e = tid; e < BK * BN; e += 256) {
+        int k, j;
+        if (b_j_fast) { j = e % BN; k = e / BN; } else { k = e % BK; j = e / BK; }
+        const long long gk = k0 + k, gj = n0 + j;
+        double v = 0.0;
+        if (gk < g.K && gj < g.N) v = __ldg(g.B + gk * g.sbk + gj * g.sbj);
+        Bs[k][j] = v;
+      }
     }
     __syncthreads();
     const int kmax = (g.K - k0) < BK ? (int)(g.K - k0) : BK;
