@@ -674,35 +674,76 @@ __global__ void __launch_bounds__(256) xgemm_kernel(XGemmArgs<E> g) {
 
   const bool a_k_fast = g.sak == 1;
   const bool b_j_fast = g.sbj == 1;
+  // whole tiles of unit-stride operands whose rows start 16-byte aligned load 16-byte
+  // vectors of VE elements
+  constexpr int PER = 16 / (int)sizeof(E), VE = PER / NC;
+  const bool a_vec = a_k_fast && ((g.sai * NC * (long long)sizeof(E)) & 15) == 0 &&
+                     ((uintptr_t)g.A & 15) == 0 && m0 + BM <= g.M;
+  const bool b_vec = b_j_fast && ((g.sbk * NC * (long long)sizeof(E)) & 15) == 0 &&
+                     ((uintptr_t)g.B & 15) == 0 && n0 + BN <= g.N;
 
 #pragma unroll 1
   for (long long k0 = 0; k0 < g.K; k0 += BK) {
+    const bool k_whole = k0 + BK <= g.K;
+    if (a_vec && k_whole) {
 #pragma unroll 1
-    for (int e = tid; e < BM * BK; e += 256) {
-      int i, k;
-      if (a_k_fast) { k = e % BK; i = e / BK; } else { i = e % BM; k = e / BM; }
-      const long long gi = m0 + i, gk = k0 + k;
-      Val<E, CX> v{E(0), E(0)};
-      if (gi < g.M && gk < g.K) {
-        v = ldv<E, CX>(g.A, gi * g.sai + gk * g.sak);
-        if (CX && g.conja) v.i = -v.i;
-        if (!g.alpha_one) v = scale<E, CX>(v, g.ar, g.ai);
+      for (int e = tid; e < BM * BK / VE; e += 256) {
+        const int i = e / (BK / VE), k = (e % (BK / VE)) * VE;
+        E raw[PER];
+        ld16<E>(g.A + ((m0 + i) * g.sai + k0 + k) * NC, raw);
+#pragma unroll
+        for (int w = 0; w < VE; w++) {
+          Val<E, CX> v;
+          v.r = raw[w * NC];
+          v.i = CX ? raw[w * NC + NC - 1] : E(0);
+          if (CX && g.conja) v.i = -v.i;
+          if (!g.alpha_one) v = scale<E, CX>(v, g.ar, g.ai);
+          As[0][k + w][i] = v.r;
+          if constexpr (CX) As[NC - 1][k + w][i] = v.i;
+        }
       }
-      As[0][k][i] = v.r;
-      if constexpr (CX) As[NC - 1][k][i] = v.i;
+    } else {
+#pragma unroll 1
+      for (int e = tid; e < BM * BK; e += 256) {
+        int i, k;
+        if (a_k_fast) { k = e % BK; i = e / BK; } else { i = e % BM; k = e / BM; }
+        const long long gi = m0 + i, gk = k0 + k;
+        Val<E, CX> v{E(0), E(0)};
+        if (gi < g.M && gk < g.K) {
+          v = ldv<E, CX>(g.A, gi * g.sai + gk * g.sak);
+          if (CX && g.conja) v.i = -v.i;
+          if (!g.alpha_one) v = scale<E, CX>(v, g.ar, g.ai);
+        }
+        As[0][k][i] = v.r;
+        if constexpr (CX) As[NC - 1][k][i] = v.i;
+      }
     }
+    if (b_vec && k_whole) {
 #pragma unroll 1
-    for (int e = tid; e < BK * BN; e += 256) {
-      int k, j;
-      if (b_j_fast) { j = e % BN; k = e / BN; } else { k = e % BK; j = e / BK; }
-      const long long gk = k0 + k, gj = n0 + j;
-      Val<E, CX> v{E(0), E(0)};
-      if (gk < g.K && gj < g.N) {
-        v = ldv<E, CX>(g.B, gk * g.sbk + gj * g.sbj);
-        if (CX && g.conjb) v.i = -v.i;
+      for (int e = tid; e < BK * BN / VE; e += 256) {
+        const int k = e / (BN / VE), j = (e % (BN / VE)) * VE;
+        E raw[PER];
+        ld16<E>(g.B + ((k0 + k) * g.sbk + n0 + j) * NC, raw);
+#pragma unroll
+        for (int w = 0; w < VE; w++) {
+          Bs[0][k][j + w] = raw[w * NC];
+          if constexpr (CX) Bs[NC - 1][k][j + w] = g.conjb ? -raw[w * NC + NC - 1] : raw[w * NC + NC - 1];
+        }
       }
-      Bs[0][k][j] = v.r;
-      if constexpr (CX) Bs[NC - 1][k][j] = v.i;
+    } else {
+#pragma unroll 1
+      for (int e = tid; e < BK * BN; e += 256) {
+        int k, j;
+        if (b_j_fast) { j = e % BN; k = e / BN; } else { k = e % BK; j = e / BK; }
+        const long long gk = k0 + k, gj = n0 + j;
+        Val<E, CX> v{E(0), E(0)};
+        if (gk < g.K && gj < g.N) {
+          v = ldv<E, CX>(g.B, gk * g.sbk + gj * g.sbj);
+          if (CX && g.conjb) v.i = -v.i;
+        }
+        Bs[0][k][j] = v.r;
+        if constexpr (CX) Bs[NC - 1][k][j] = v.i;
+      }
     }
     __syncthreads();
     const int kmax = (g.K - k0) < BK ? (int)(g.K - k0) : BK;
