@@ -388,7 +388,9 @@ __device__ __forceinline__ void lds_row(const double* p, double (&v)[TN]) {
 // non-finite branch: the tile's products are deposited without per-product checks, exactly
 // as the per-step fast path (tileN) would deposit them. Otherwise the tile takes the
 // per-step path. Both give the same state.
-template <int F, int TM, int TN>
+// PIPE: whole K tiles of pair-loading operands are prefetched into registers (the plain
+// dgemm kernel; the batched kernel's tiles keep the registers for occupancy).
+template <int F, int TM, int TN, bool PIPE = false>
 __device__ __forceinline__ void gemm_tile(const GemmArgs& g, long long m0, long long n0) {
   using Cfg = GemmCfg<F, TM, TN>;
   using B = BT<double>;
@@ -411,12 +413,48 @@ __device__ __forceinline__ void gemm_tile(const GemmArgs& g, long long m0, long 
   // load 16-byte pairs
   const bool a_pairs = a_k_fast && (g.sai & 1) == 0 && ((uintptr_t)g.A & 15) == 0 && m0 + BM <= g.M;
   const bool b_pairs = b_j_fast && (g.sbk & 1) == 0 && ((uintptr_t)g.B & 15) == 0 && n0 + BN <= g.N;
+  // When every K tile is whole and both operands load pairs, the next K tile's pairs are
+  // loaded into registers while the current one is deposited.
+  constexpr int APV = BM * BK / 2 / 256, BPV = BK * BN / 2 / 256;   // pairs per thread
+  static_assert(APV * 512 == BM * BK && BPV * 512 == BK * BN, "pair split");
+  const bool pipe = PIPE && a_pairs && b_pairs && g.K % BK == 0;
+  double2 pa[APV], pb[BPV];
+  auto fetch = [&](long long k0) {
+#pragma unroll
+    for (int u = 0; u < APV; u++) {
+      const int e = tid + 256 * u, i = e / (BK / 2), k = 2 * (e % (BK / 2));
+      pa[u] = __ldg((const double2*)(g.A + (m0 + i) * g.sai + k0 + k));
+    }
+#pragma unroll
+    for (int u = 0; u < BPV; u++) {
+      const int e = tid + 256 * u, k = e / (BN / 2), j = 2 * (e % (BN / 2));
+      pb[u] = __ldg((const double2*)(g.B + (k0 + k) * g.sbk + n0 + j));
+    }
+  };
+  if (pipe) fetch(0);
 
 #pragma unroll 1
   for (long long k0 = 0; k0 < g.K; k0 += BK) {
     const bool k_whole = k0 + BK <= g.K;
-    // A tile: BM x BK
-    if (a_pairs && k_whole) {
+    if (pipe) {
+#pragma unroll
+      for (int u = 0; u < APV; u++) {
+        const int e = tid + 256 * u, i = e / (BK / 2), k = 2 * (e % (BK / 2));
+        double v0 = pa[u].x, v1 = pa[u].y;
+        if (g.alpha != 1.0) {
+          v0 = __dmul_rn(v0, g.alpha);
+          v1 = __dmul_rn(v1, g.alpha);
+        }
+        As[k][i] = v0;
+        As[k + 1][i] = v1;
+      }
+#pragma unroll
+      for (int u = 0; u < BPV; u++) {
+        const int e = tid + 256 * u, k = e / (BN / 2), j = 2 * (e % (BN / 2));
+        *(double2*)&Bs[k][j] = pb[u];
+      }
+      if (k0 + BK < g.K) fetch(k0 + BK);
+    } else if (a_pairs && k_whole) {
 #pragma unroll 1
       for (int e = tid; e < BM * BK / 2; e += 256) {
         const int i = e / (BK / 2), k = 2 * (e % (BK / 2));
@@ -444,7 +482,9 @@ __device__ __forceinline__ void gemm_tile(const GemmArgs& g, long long m0, long 
       }
     }
     // B tile: BK x BN
-    if (b_pairs && k_whole) {
+    if (pipe) {
+      // stored above
+    } else if (b_pairs && k_whole) {
 #pragma unroll 1
       for (int e = tid; e < BK * BN / 2; e += 256) {
         const int k = e / (BN / 2), j = 2 * (e % (BN / 2));
@@ -542,9 +582,9 @@ __device__ __forceinline__ void gemm_tile(const GemmArgs& g, long long m0, long 
 }
 
 template <int F, int TM, int TN>
-__global__ void __launch_bounds__(256) gemm_kernel(GemmArgs g) {
+__global__ void __launch_bounds__(256, 2) gemm_kernel(GemmArgs g) {
   using Cfg = GemmCfg<F, TM, TN>;
-  gemm_tile<F, TM, TN>(g, (long long)blockIdx.y * Cfg::BM, (long long)blockIdx.x * Cfg::BN);
+  gemm_tile<F, TM, TN, true>(g, (long long)blockIdx.y * Cfg::BM, (long long)blockIdx.x * Cfg::BN);
 }
 
 template <int F>
